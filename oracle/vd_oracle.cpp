@@ -1,0 +1,1658 @@
+// CPU ORACLE -- test infrastructure only, never part of the product path.
+//
+// A plain FP64 C++17 (OpenMP) restatement of the reference's per-timestep
+// species-and-field update on one uniform level, used by tests/, by
+// __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the checker
+// of the CUDA library.  It is built once per case directory, like the
+// library, and exports vdo_* functions mirroring include/vidyut_b200.h.
+//
+// It follows, function by function:
+//   Source/Evolve.cpp:136-617          step order, Sborder/Sborder_old use,
+//                                      corrector midpoint average
+//   Source/PotentialSolve.cpp:19-554   solve_potential
+//   Source/ScalarSolve.cpp:17-329      compute_dsdt, rxn/expl sources,
+//                                      transport fluxes
+//   Source/ScalarSolve.cpp:380-1000    implicit_solve_scalar
+//   Source/compute_explicit_flux.H     weno / WAF / upwind, compute_flux
+//   Source/ElecEnergySource.cpp:17-294 LFA electron temperature, Joule heating
+//   Source/HelperFuncs.H:13-161        one-sided gradient, applied potential
+//   Source/Vidyut.cpp:116-130          foextrap / int_dir ghost fill
+//
+// The linear solves are a restatement of the published behaviour of AMReX's
+// MLABecLaplacian + MLMG (third party, absent from the reference checkout:
+// `Submodules/amrex` is an empty submodule, pinned commit unrecoverable):
+// cell-centred (A a - B div(b grad)) operator, ghost-cell boundary closure
+// (Dirichlet by polynomial extrapolation of order `maxorder`, homogeneous
+// Neumann by reflection, inhomogeneous Neumann through the right-hand side,
+// Robin a*phi + b*dphi/dn = f), red-black Gauss-Seidel smoothing,
+// 2x averaging restriction, piecewise-constant prolongation, V-cycles on the
+// correction equation, BiCGStab bottom solve (rel 1e-4, 200 iterations,
+// then `nub` smooths, or `nuf` smooths on failure), max-norm convergence
+// test |r| <= max(tol_abs, tol_rel |r0|).  Harmonic face averaging of cell
+// coefficients returns 0 where both cells are 0.
+//
+// Parity status: the discretisation is pinned by the reference's own
+// known-answer tests (MMS1 steady state, Advect WENO5 convergence) through
+// tests/test_oracle_known_answers.py; iteration-level agreement with MLMG
+// is unpinned because AMReX is not available to run here.
+#include <vidyut_b200.h>
+
+#include "vd_vars.H"
+#include "vd_parmparse.H"
+#include "PlasmaChem.H"
+#include <UserFunctions.H>
+#include <UserSources.H>
+#include <Prob.H>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+using vd::Array4;
+using vd::GpuArray;
+using vd::IntVect;
+using vd::Real;
+
+namespace {
+
+// ------------------------------------------------------------------ grids
+struct Geom
+{
+    int dim = 3;
+    int n[3] = {1, 1, 1};
+    Real dx[3] = {1, 1, 1};
+    Real lo[3] = {0, 0, 0};
+    Real hi[3] = {1, 1, 1};
+    int per[3] = {0, 0, 0};
+    long long ncell() const { return (long long)n[0] * n[1] * n[2]; }
+};
+
+// A cell-centred array with `ng` ghost layers in the active directions.
+struct Fab
+{
+    int n[3] = {1, 1, 1};
+    int g[3] = {0, 0, 0};
+    int ncomp = 1;
+    long long sx = 0, sy = 0, sz = 0, sc = 0;
+    std::vector<Real> d;
+
+    void define(const Geom& geo, int ncomp_, int ng)
+    {
+        ncomp = ncomp_;
+        for (int a = 0; a < 3; ++a)
+        {
+            n[a] = geo.n[a];
+            g[a] = (a < geo.dim) ? ng : 0;
+        }
+        sx = n[0] + 2 * g[0];
+        sy = n[1] + 2 * g[1];
+        sz = n[2] + 2 * g[2];
+        sc = sx * sy * sz;
+        d.assign(sc * ncomp, 0.0);
+    }
+    Real& operator()(int i, int j, int k, int c = 0)
+    {
+        return d[(i + g[0]) + sx * ((j + g[1]) + sy * (k + g[2])) + sc * c];
+    }
+    Real operator()(int i, int j, int k, int c = 0) const
+    {
+        return d[(i + g[0]) + sx * ((j + g[1]) + sy * (k + g[2])) + sc * c];
+    }
+    Array4 view()
+    {
+        Array4 a;
+        a.p = d.data();
+        for (int q = 0; q < 3; ++q)
+        {
+            a.lo[q] = -g[q];
+            a.hi[q] = n[q] - 1 + g[q];
+        }
+        a.jstride = sx;
+        a.kstride = sx * sy;
+        a.nstride = sc;
+        return a;
+    }
+    void setVal(Real v) { std::fill(d.begin(), d.end(), v); }
+};
+
+// Face-centred array in direction `dir` (n[dir]+1 faces).
+struct FaceFab
+{
+    int n[3] = {1, 1, 1};
+    int ncomp = 1;
+    std::vector<Real> d;
+    void define(const Geom& geo, int dir, int ncomp_)
+    {
+        ncomp = ncomp_;
+        for (int a = 0; a < 3; ++a) n[a] = geo.n[a] + (a == dir ? 1 : 0);
+        d.assign((size_t)n[0] * n[1] * n[2] * ncomp, 0.0);
+    }
+    Real& operator()(int i, int j, int k, int c = 0)
+    {
+        return d[i + (size_t)n[0] * (j + (size_t)n[1] * (k + (size_t)n[2] * c))];
+    }
+};
+
+// FillPatch on one level: valid cells copied, ghost cells by foextrap (clamp)
+// or periodic wrap, dimension by dimension (Source/Vidyut.cpp:116-130).
+void fill_patch(const Geom& geo, const Fab& src, Fab& dst, int ncomp)
+{
+    const int g0 = dst.g[0], g1 = dst.g[1], g2 = dst.g[2];
+    auto fix = [&](int i, int a) {
+        const int n = geo.n[a];
+        if (i < 0) return geo.per[a] ? ((i % n) + n) % n : 0;
+        if (i >= n) return geo.per[a] ? i % n : n - 1;
+        return i;
+    };
+#pragma omp parallel for collapse(2)
+    for (int c = 0; c < ncomp; ++c)
+        for (int k = -g2; k < geo.n[2] + g2; ++k)
+            for (int j = -g1; j < geo.n[1] + g1; ++j)
+                for (int i = -g0; i < geo.n[0] + g0; ++i)
+                    dst(i, j, k, c) = src(fix(i, 0), fix(j, 1), fix(k, 2), c);
+}
+
+// -------------------------------------------------- drift-flux numerics
+// Restatement of Source/compute_explicit_flux.H:16-214.
+Real o_gk(Real wk, Real g)
+{
+    return wk * (g + g * g - 3.0 * g * wk + wk * wk) /
+           (g * g + wk * (1 - 2.0 * g));
+}
+
+Real o_weno(Real a, Real b, Real c, Real d, Real e, int scheme)
+{
+    const Real eps = 1e-20;
+    const Real p1 = (1.0 / 3.0) * a - (7.0 / 6.0) * b + (11.0 / 6.0) * c;
+    const Real p2 = -(1.0 / 6.0) * b + (5.0 / 6.0) * c + (1.0 / 3.0) * d;
+    const Real p3 = (1.0 / 3.0) * c + (5.0 / 6.0) * d - (1.0 / 6.0) * e;
+    const Real t1 = a - 2.0 * b + c, t1b = a - 4.0 * b + 3.0 * c;
+    const Real t2 = b - 2.0 * c + d, t2b = b - d;
+    const Real t3 = c - 2.0 * d + e, t3b = 3.0 * c - 4.0 * d + e;
+    const Real b1 = (13.0 / 12.0) * t1 * t1 + 0.25 * t1b * t1b;
+    const Real b2 = (13.0 / 12.0) * t2 * t2 + 0.25 * t2b * t2b;
+    const Real b3 = (13.0 / 12.0) * t3 * t3 + 0.25 * t3b * t3b;
+    const Real g1 = 0.1, g2 = 0.6, g3 = 0.3;
+    Real a1, a2, a3;
+    if (scheme == 1 || scheme == 2)
+    {
+        a1 = g1 / ((b1 + eps) * (b1 + eps));
+        a2 = g2 / ((b2 + eps) * (b2 + eps));
+        a3 = g3 / ((b3 + eps) * (b3 + eps));
+        if (scheme == 2)
+        {
+            const Real s = a1 + a2 + a3;
+            const Real w1 = a1 / s, w2 = a2 / s, w3 = a3 / s;
+            a1 = o_gk(w1, g1);
+            a2 = o_gk(w2, g2);
+            a3 = o_gk(w3, g3);
+        }
+    } else
+    {
+        const Real tau = std::fabs(b1 - b3);
+        const Real r1 = tau / (b1 + eps), r2 = tau / (b2 + eps),
+                   r3 = tau / (b3 + eps);
+        a1 = g1 * (1.0 + r1 * r1);
+        a2 = g2 * (1.0 + r2 * r2);
+        a3 = g3 * (1.0 + r3 * r3);
+    }
+    const Real s = a1 + a2 + a3;
+    return (a1 / s) * p1 + (a2 / s) * p2 + (a3 / s) * p3;
+}
+
+Real o_minbee(Real c, Real dl, Real dm, Real dr)
+{
+    const Real heps = 1.0e-30;
+    const Real r = (c >= 0.0) ? dl / (dm + heps) : dr / (dm + heps);
+    if (r <= 0.0) return 1.0;
+    if (r <= 1.0) return 1.0 - (1.0 - std::fabs(c)) * r;
+    return std::fabs(c);
+}
+
+Real o_waf(Real vL, Real vR, Real pLm1, Real pL, Real pR, Real pRp1, Real dx,
+           Real dt)
+{
+    const Real vm = 0.5 * (vL + vR);
+    const Real sgn = std::copysign(1.0, vm);
+    const Real c = vm * dt / dx;
+    const Real fL = pL * vL, fR = pR * vR;
+    const Real lim = o_minbee(c, pL - pLm1, pR - pL, pRp1 - pR);
+    return 0.5 * (fL + fR) - 0.5 * sgn * lim * (fR - fL);
+}
+
+Real o_upwind(Real vL, Real vR, Real pL, Real pR)
+{
+    const Real vm = 0.5 * (vL + vR);
+    const Real sgn = std::copysign(1.0, vm);
+    return pL * vL * 0.5 * (1.0 + sgn) + pR * vR * 0.5 * (1.0 - sgn);
+}
+
+// ------------------------------------------------ multigrid (MLMG restated)
+enum OBC
+{
+    O_PER,
+    O_DIR,
+    O_NEU,
+    O_INNEU,
+    O_ROBIN
+};
+
+int map_bc(int code)
+{
+    switch (code)
+    {
+    case PERBC: return O_PER;
+    case DIRCBC: return O_DIR;
+    case HNEUBC: return O_NEU;
+    case IHNEUBC: return O_INNEU;
+    case ROBINBC: return O_ROBIN;
+    case AXISBC: return O_NEU;
+    default: return O_ROBIN;
+    }
+}
+
+struct Side
+{
+    int type = O_NEU;
+    // per boundary face (tangential plane), fine level only
+    std::vector<Real> val, ra, rb, rf;
+};
+
+struct OLevel
+{
+    Geom geo;
+    std::vector<Real> a;           // cell coefficient
+    std::vector<Real> b[3];        // face coefficients
+    std::vector<Real> cor, res, rescor;
+    std::vector<Real> ra[6], rb[6]; // Robin a,b on this level's boundary faces
+};
+
+struct OMG
+{
+    int dim = 3;
+    int maxorder = 3;
+    Real alpha = 0, beta = 1;
+    std::vector<OLevel> L;
+    int type[6];
+    std::vector<Real> bval[6]; // inhomogeneous boundary values (fine)
+    std::vector<Real> rf[6];   // Robin f (fine)
+    int nu1 = 2, nu2 = 2, nuf = 8, nub = 0, maxiter = 100;
+    Real bot_rel = 1e-4;
+    int bot_maxiter = 200;
+
+    static long long idx(const Geom& g, int i, int j, int k)
+    {
+        return i + (long long)g.n[0] * (j + (long long)g.n[1] * k);
+    }
+    static long long fidx(const Geom& g, int d, int i, int j, int k)
+    {
+        const int nx = g.n[0] + (d == 0), ny = g.n[1] + (d == 1);
+        return i + (long long)nx * (j + (long long)ny * k);
+    }
+    static int plane(const Geom& g, int d, int i, int j, int k)
+    {
+        if (d == 0) return j + g.n[1] * k;
+        if (d == 1) return i + g.n[0] * k;
+        return i + g.n[0] * j;
+    }
+    static int plane_size(const Geom& g, int d)
+    {
+        if (d == 0) return g.n[1] * g.n[2];
+        if (d == 1) return g.n[0] * g.n[2];
+        return g.n[0] * g.n[1];
+    }
+
+    // Ghost value outside side s (d = s%3, hi = s/3) next to interior cell
+    // (i,j,k) of level l.  `inhomog` selects the fine-level boundary data.
+    Real ghost(int l, int s, const std::vector<Real>& x, int i, int j, int k,
+               bool inhomog) const
+    {
+        const Geom& g = L[l].geo;
+        const int d = s % 3, hiside = s / 3;
+        const int p = plane(g, d, i, j, k);
+        const int sg = hiside ? -1 : 1; // direction into the domain
+        const Real x0 = x[idx(g, i, j, k)];
+        switch (type[s])
+        {
+        case O_NEU:
+        case O_INNEU: return x0;
+        case O_DIR:
+        {
+            int nx = std::min(g.n[d] + 1, maxorder);
+            const Real bv = inhomog ? bval[s][p] : 0.0;
+            if (nx <= 2) return 2.0 * bv - x0;
+            int ii = i, jj = j, kk = k;
+            (d == 0 ? ii : (d == 1 ? jj : kk)) += sg;
+            const Real x1 = x[idx(g, ii, jj, kk)];
+            return (8.0 / 3.0) * bv - 2.0 * x0 + (1.0 / 3.0) * x1;
+        }
+        case O_ROBIN:
+        {
+            const Real a = L[l].ra[s][p], b = L[l].rb[s][p];
+            const Real dxi = 1.0 / g.dx[d];
+            const Real f = inhomog ? rf[s][p] : 0.0;
+            return (f + x0 * (b * dxi - 0.5 * a)) / (0.5 * a + b * dxi);
+        }
+        default: return x0;
+        }
+    }
+    // Coefficient of the interior cell in the ghost expression (the
+    // "undrrelxr" factor the Gauss-Seidel diagonal absorbs).
+    Real ghost_coef(int l, int s, int i, int j, int k) const
+    {
+        const Geom& g = L[l].geo;
+        const int d = s % 3;
+        switch (type[s])
+        {
+        case O_NEU:
+        case O_INNEU: return 1.0;
+        case O_DIR: return (std::min(g.n[d] + 1, maxorder) <= 2) ? -1.0 : -2.0;
+        case O_ROBIN:
+        {
+            const int p = plane(g, d, i, j, k);
+            const Real a = L[l].ra[s][p], b = L[l].rb[s][p];
+            const Real dxi = 1.0 / g.dx[d];
+            return (b * dxi - 0.5 * a) / (0.5 * a + b * dxi);
+        }
+        default: return 0.0;
+        }
+    }
+
+    // Neighbour of (i,j,k) one step along d in direction sg.
+    Real nbr(int l, const std::vector<Real>& x, int i, int j, int k, int d,
+             int sg, bool inhomog) const
+    {
+        const Geom& g = L[l].geo;
+        int c[3] = {i, j, k};
+        c[d] += sg;
+        if (c[d] < 0 || c[d] >= g.n[d])
+        {
+            if (g.per[d])
+            {
+                c[d] = (c[d] + g.n[d]) % g.n[d];
+                return x[idx(g, c[0], c[1], c[2])];
+            }
+            return ghost(l, d + (sg > 0 ? 3 : 0), x, i, j, k, inhomog);
+        }
+        return x[idx(g, c[0], c[1], c[2])];
+    }
+
+    Real Lx(int l, const std::vector<Real>& x, int i, int j, int k,
+            bool inhomog) const
+    {
+        const OLevel& lv = L[l];
+        const Geom& g = lv.geo;
+        const Real x0 = x[idx(g, i, j, k)];
+        Real y = alpha * lv.a[idx(g, i, j, k)] * x0;
+        for (int d = 0; d < dim; ++d)
+        {
+            const Real dh = beta / (g.dx[d] * g.dx[d]);
+            int c[3] = {i, j, k};
+            const Real blo = lv.b[d][fidx(g, d, c[0], c[1], c[2])];
+            c[d] += 1;
+            const Real bhi = lv.b[d][fidx(g, d, c[0], c[1], c[2])];
+            const Real xm = nbr(l, x, i, j, k, d, -1, inhomog);
+            const Real xp = nbr(l, x, i, j, k, d, +1, inhomog);
+            y -= dh * (bhi * (xp - x0) - blo * (x0 - xm));
+        }
+        return y;
+    }
+
+    void residual(int l, const std::vector<Real>& x, const std::vector<Real>& f,
+                  std::vector<Real>& r, bool inhomog) const
+    {
+        const Geom& g = L[l].geo;
+#pragma omp parallel for collapse(2)
+        for (int k = 0; k < g.n[2]; ++k)
+            for (int j = 0; j < g.n[1]; ++j)
+                for (int i = 0; i < g.n[0]; ++i)
+                    r[idx(g, i, j, k)] =
+                        f[idx(g, i, j, k)] - Lx(l, x, i, j, k, inhomog);
+    }
+
+    // One red-black Gauss-Seidel smooth (red sweep then black sweep).
+    void smooth(int l, std::vector<Real>& x, const std::vector<Real>& f,
+                bool inhomog) const
+    {
+        const OLevel& lv = L[l];
+        const Geom& g = lv.geo;
+        for (int color = 0; color < 2; ++color)
+        {
+#pragma omp parallel for collapse(2)
+            for (int k = 0; k < g.n[2]; ++k)
+                for (int j = 0; j < g.n[1]; ++j)
+                    for (int i = 0; i < g.n[0]; ++i)
+                    {
+                        if ((i + j + k + color) % 2 != 0) continue;
+                        const long long p = idx(g, i, j, k);
+                        Real gamma = alpha * lv.a[p];
+                        Real rho = 0.0, delta = 0.0;
+                        for (int d = 0; d < dim; ++d)
+                        {
+                            const Real dh = beta / (g.dx[d] * g.dx[d]);
+                            int c[3] = {i, j, k};
+                            const Real blo = lv.b[d][fidx(g, d, c[0], c[1], c[2])];
+                            c[d] += 1;
+                            const Real bhi = lv.b[d][fidx(g, d, c[0], c[1], c[2])];
+                            gamma += dh * (blo + bhi);
+                            rho += dh * (blo * nbr(l, x, i, j, k, d, -1, inhomog) +
+                                         bhi * nbr(l, x, i, j, k, d, +1, inhomog));
+                            int cc[3] = {i, j, k};
+                            if (!g.per[d] && cc[d] == 0)
+                                delta += dh * blo * ghost_coef(l, d, i, j, k);
+                            if (!g.per[d] && cc[d] == g.n[d] - 1)
+                                delta += dh * bhi * ghost_coef(l, d + 3, i, j, k);
+                        }
+                        const Real res = f[p] - (gamma * x[p] - rho);
+                        x[p] = x[p] + res / (gamma - delta);
+                    }
+        }
+    }
+
+    static Real norminf(const std::vector<Real>& v)
+    {
+        Real m = 0.0;
+#pragma omp parallel for reduction(max : m)
+        for (long long q = 0; q < (long long)v.size(); ++q)
+            m = std::max(m, std::fabs(v[q]));
+        return m;
+    }
+
+    void restrict_to(int l, const std::vector<Real>& fine, std::vector<Real>& crse) const
+    {
+        const Geom& gc = L[l + 1].geo;
+        const Geom& gf = L[l].geo;
+        const int rz = (dim == 3) ? 2 : 1;
+        const Real w = (dim == 3) ? 0.125 : 0.25;
+#pragma omp parallel for collapse(2)
+        for (int k = 0; k < gc.n[2]; ++k)
+            for (int j = 0; j < gc.n[1]; ++j)
+                for (int i = 0; i < gc.n[0]; ++i)
+                {
+                    Real s = 0.0;
+                    for (int kk = 0; kk < rz; ++kk)
+                        for (int jj = 0; jj < 2; ++jj)
+                            for (int ii = 0; ii < 2; ++ii)
+                                s += fine[idx(gf, 2 * i + ii, 2 * j + jj, rz * k + kk)];
+                    crse[idx(gc, i, j, k)] = s * w;
+                }
+    }
+
+    void prolong_add(int l, std::vector<Real>& fine, const std::vector<Real>& crse) const
+    {
+        const Geom& gf = L[l].geo;
+        const Geom& gc = L[l + 1].geo;
+        const int rz = (dim == 3) ? 2 : 1;
+#pragma omp parallel for collapse(2)
+        for (int k = 0; k < gf.n[2]; ++k)
+            for (int j = 0; j < gf.n[1]; ++j)
+                for (int i = 0; i < gf.n[0]; ++i)
+                    fine[idx(gf, i, j, k)] += crse[idx(gc, i / 2, j / 2, k / rz)];
+    }
+
+    // BiCGStab on the coarsest level (homogeneous boundaries).
+    int bicgstab(int l, std::vector<Real>& x, const std::vector<Real>& b) const
+    {
+        const Geom& g = L[l].geo;
+        const long long n = g.ncell();
+        std::vector<Real> r(n), rh(n), p(n, 0.0), v(n, 0.0), s(n), t(n), tmp(n);
+        std::fill(x.begin(), x.end(), 0.0);
+        r = b;
+        const Real rnorm0 = norminf(r);
+        if (rnorm0 == 0.0) return 0;
+        rh = r;
+        Real rho_1 = 0, alpha_ = 0, omega = 0;
+        auto dot = [&](const std::vector<Real>& u, const std::vector<Real>& w) {
+            Real acc = 0.0;
+            for (long long q = 0; q < n; ++q) acc += u[q] * w[q];
+            return acc;
+        };
+        auto apply = [&](const std::vector<Real>& in, std::vector<Real>& out) {
+            for (int k = 0; k < g.n[2]; ++k)
+                for (int j = 0; j < g.n[1]; ++j)
+                    for (int i = 0; i < g.n[0]; ++i)
+                        out[idx(g, i, j, k)] = Lx(l, in, i, j, k, false);
+        };
+        for (int iter = 1; iter <= bot_maxiter; ++iter)
+        {
+            const Real rho = dot(rh, r);
+            if (rho == 0.0) return 1;
+            if (iter == 1)
+                p = r;
+            else
+            {
+                const Real bet = (rho / rho_1) * (alpha_ / omega);
+                for (long long q = 0; q < n; ++q) p[q] = r[q] + bet * (p[q] - omega * v[q]);
+            }
+            apply(p, v);
+            const Real rhTv = dot(rh, v);
+            if (rhTv == 0.0) return 2;
+            alpha_ = rho / rhTv;
+            for (long long q = 0; q < n; ++q)
+            {
+                x[q] += alpha_ * p[q];
+                s[q] = r[q] - alpha_ * v[q];
+            }
+            if (norminf(s) <= bot_rel * rnorm0) return 0;
+            apply(s, t);
+            const Real tt = dot(t, t);
+            if (tt == 0.0) return 3;
+            omega = dot(t, s) / tt;
+            for (long long q = 0; q < n; ++q)
+            {
+                x[q] += omega * s[q];
+                r[q] = s[q] - omega * t[q];
+            }
+            if (norminf(r) <= bot_rel * rnorm0) return 0;
+            if (omega == 0.0) return 4;
+            rho_1 = rho;
+        }
+        return 8;
+    }
+
+    void vcycle()
+    {
+        const int nl = (int)L.size();
+        for (int l = 0; l < nl - 1; ++l)
+        {
+            if (l > 0) std::fill(L[l].cor.begin(), L[l].cor.end(), 0.0);
+            for (int s = 0; s < nu1; ++s) smooth(l, L[l].cor, L[l].res, false);
+            residual(l, L[l].cor, L[l].res, L[l].rescor, false);
+            restrict_to(l, L[l].rescor, L[l + 1].res);
+        }
+        {
+            const int l = nl - 1;
+            if (nl == 1)
+            {
+                for (int s = 0; s < nuf; ++s) smooth(l, L[l].cor, L[l].res, false);
+            } else
+            {
+                const int ret = bicgstab(l, L[l].cor, L[l].res);
+                const int ns = (ret == 0) ? nub : nuf;
+                for (int s = 0; s < ns; ++s) smooth(l, L[l].cor, L[l].res, false);
+            }
+        }
+        for (int l = nl - 2; l >= 0; --l)
+        {
+            prolong_add(l, L[l].cor, L[l + 1].cor);
+            for (int s = 0; s < nu2; ++s) smooth(l, L[l].cor, L[l].res, false);
+        }
+    }
+
+    // Build the level hierarchy: halve every active direction while it stays
+    // even and at least 2 cells, up to `maxlev` coarsenings.
+    void build(const Geom& fine, int maxlev)
+    {
+        L.clear();
+        L.emplace_back();
+        L[0].geo = fine;
+        while ((int)L.size() - 1 < maxlev)
+        {
+            const Geom& g = L.back().geo;
+            bool ok = true;
+            for (int d = 0; d < dim; ++d)
+                if (g.n[d] % 2 != 0 || g.n[d] / 2 < 2) ok = false;
+            if (!ok) break;
+            Geom c = g;
+            for (int d = 0; d < dim; ++d)
+            {
+                c.n[d] = g.n[d] / 2;
+                c.dx[d] = g.dx[d] * 2.0;
+            }
+            L.emplace_back();
+            L.back().geo = c;
+        }
+        for (auto& lv : L)
+        {
+            const long long n = lv.geo.ncell();
+            lv.a.assign(n, 0.0);
+            for (int d = 0; d < 3; ++d)
+            {
+                const int nx = lv.geo.n[0] + (d == 0), ny = lv.geo.n[1] + (d == 1),
+                          nz = lv.geo.n[2] + (d == 2);
+                lv.b[d].assign((size_t)nx * ny * nz, 0.0);
+            }
+            lv.cor.assign(n, 0.0);
+            lv.res.assign(n, 0.0);
+            lv.rescor.assign(n, 0.0);
+            for (int s = 0; s < 6; ++s)
+            {
+                lv.ra[s].assign(plane_size(lv.geo, s % 3), 0.0);
+                lv.rb[s].assign(plane_size(lv.geo, s % 3), 1.0);
+            }
+        }
+        for (int s = 0; s < 6; ++s)
+        {
+            bval[s].assign(plane_size(fine, s % 3), 0.0);
+            rf[s].assign(plane_size(fine, s % 3), 0.0);
+        }
+    }
+
+    // Average the fine-level coefficients down the hierarchy: cells by the
+    // 2^dim mean, faces by the mean of the 2^(dim-1) coincident fine faces.
+    void average_down_coeffs()
+    {
+        const int rz = (dim == 3) ? 2 : 1;
+        for (size_t l = 1; l < L.size(); ++l)
+        {
+            const Geom& gf = L[l - 1].geo;
+            const Geom& gc = L[l].geo;
+            restrict_to((int)l - 1, L[l - 1].a, L[l].a);
+            for (int d = 0; d < dim; ++d)
+            {
+                const int nx = gc.n[0] + (d == 0), ny = gc.n[1] + (d == 1),
+                          nz = gc.n[2] + (d == 2);
+                for (int k = 0; k < nz; ++k)
+                    for (int j = 0; j < ny; ++j)
+                        for (int i = 0; i < nx; ++i)
+                        {
+                            Real s = 0.0;
+                            int cnt = 0;
+                            for (int kk = 0; kk < (d == 2 ? 1 : rz); ++kk)
+                                for (int jj = 0; jj < (d == 1 ? 1 : 2); ++jj)
+                                    for (int ii = 0; ii < (d == 0 ? 1 : 2); ++ii)
+                                    {
+                                        const int fi = (d == 0) ? 2 * i : 2 * i + ii;
+                                        const int fj = (d == 1) ? 2 * j : 2 * j + jj;
+                                        const int fk = (d == 2) ? 2 * k : rz * k + kk;
+                                        s += L[l - 1].b[d][fidx(gf, d, fi, fj, fk)];
+                                        ++cnt;
+                                    }
+                            L[l].b[d][fidx(gc, d, i, j, k)] = s / cnt;
+                        }
+            }
+            for (int s = 0; s < 6; ++s)
+            {
+                const int d = s % 3;
+                const int ta = (d == 0) ? 1 : 0, tb = (d == 2) ? 1 : 2;
+                const int na = gc.n[ta], nb = gc.n[tb];
+                for (int q = 0; q < na * nb; ++q)
+                {
+                    const int ia = q % na, ib = q / na;
+                    Real sa = 0.0, sb = 0.0;
+                    int cnt = 0;
+                    for (int u = 0; u < 2; ++u)
+                        for (int w = 0; w < ((tb < dim) ? 2 : 1); ++w)
+                        {
+                            const int fa = 2 * ia + u;
+                            const int fb = (tb < dim) ? 2 * ib + w : ib;
+                            const int fp = fa + gf.n[ta] * fb;
+                            sa += L[l - 1].ra[s][fp];
+                            sb += L[l - 1].rb[s][fp];
+                            ++cnt;
+                        }
+                    L[l].ra[s][q] = sa / cnt;
+                    L[l].rb[s][q] = sb / cnt;
+                }
+            }
+        }
+    }
+
+    // rhs adjustment of inhomogeneous Neumann faces: the normal gradient
+    // enters the right-hand side, the operator keeps a reflecting ghost.
+    void apply_inhomog_neumann(std::vector<Real>& rhs) const
+    {
+        const Geom& g = L[0].geo;
+        for (int s = 0; s < 6; ++s)
+        {
+            if (type[s] != O_INNEU) continue;
+            const int d = s % 3, hiside = s / 3;
+            const Real fac = beta / g.dx[d];
+            for (int k = 0; k < g.n[2]; ++k)
+                for (int j = 0; j < g.n[1]; ++j)
+                    for (int i = 0; i < g.n[0]; ++i)
+                    {
+                        const int c[3] = {i, j, k};
+                        if (c[d] != (hiside ? g.n[d] - 1 : 0)) continue;
+                        int f[3] = {i, j, k};
+                        if (hiside) f[d] += 1;
+                        const Real b = L[0].b[d][fidx(g, d, f[0], f[1], f[2])];
+                        const Real gv = bval[s][plane(g, d, i, j, k)];
+                        rhs[idx(g, i, j, k)] += (hiside ? 1.0 : -1.0) * fac * b * gv;
+                    }
+        }
+    }
+
+    // Solve L(sol) = rhs; returns iterations, -1 when maxiter is hit.
+    int solve(std::vector<Real>& sol, std::vector<Real> rhs, Real tol_rel,
+              Real tol_abs, vd_solve_stats* st)
+    {
+        apply_inhomog_neumann(rhs);
+        OLevel& f = L[0];
+        residual(0, sol, rhs, f.res, true);
+        const Real r0 = norminf(f.res);
+        // relative to the larger of |rhs| and |r0| (MLMG's "bnorm"/"resid0")
+        const Real b0 = norminf(rhs);
+        const Real target = std::max(tol_abs, std::max(tol_rel, 1e-16) * std::max(b0, r0));
+        if (st)
+        {
+            st->initial_residual = r0;
+            st->final_residual = r0;
+            st->iterations = 0;
+            st->converged = 1;
+        }
+        if (r0 <= target) return 0;
+        for (int it = 1; it <= maxiter; ++it)
+        {
+            std::fill(f.cor.begin(), f.cor.end(), 0.0);
+            vcycle();
+            for (size_t q = 0; q < sol.size(); ++q) sol[q] += f.cor[q];
+            residual(0, sol, rhs, f.res, true);
+            const Real rn = norminf(f.res);
+            if (st)
+            {
+                st->final_residual = rn;
+                st->iterations = it;
+            }
+            if (rn <= target) return it;
+        }
+        if (st) st->converged = 0;
+        return -1;
+    }
+
+    // Face gradient of `sol` with inhomogeneous boundary ghosts (MLMG
+    // getGradSolution); inhomogeneous-Neumann faces return their gradient.
+    void grad(const std::vector<Real>& sol, FaceFab* out) const
+    {
+        const Geom& g = L[0].geo;
+        for (int d = 0; d < dim; ++d)
+        {
+            const Real dxi = 1.0 / g.dx[d];
+            FaceFab& F = out[d];
+            for (int k = 0; k < F.n[2]; ++k)
+                for (int j = 0; j < F.n[1]; ++j)
+                    for (int i = 0; i < F.n[0]; ++i)
+                    {
+                        int c[3] = {i, j, k};
+                        const int fi = c[d];
+                        if (fi > 0 && fi < g.n[d])
+                        {
+                            int m[3] = {i, j, k};
+                            m[d] -= 1;
+                            F(i, j, k) = (sol[idx(g, i, j, k)] - sol[idx(g, m[0], m[1], m[2])]) * dxi;
+                            continue;
+                        }
+                        if (g.per[d])
+                        {
+                            int m[3] = {i, j, k}, p[3] = {i, j, k};
+                            m[d] = g.n[d] - 1;
+                            p[d] = 0;
+                            F(i, j, k) = (sol[idx(g, p[0], p[1], p[2])] - sol[idx(g, m[0], m[1], m[2])]) * dxi;
+                            continue;
+                        }
+                        const bool lo = (fi == 0);
+                        int in[3] = {i, j, k};
+                        if (!lo) in[d] -= 1;
+                        const int s = d + (lo ? 0 : 3);
+                        if (type[s] == O_INNEU)
+                        {
+                            F(i, j, k) = bval[s][plane(g, d, in[0], in[1], in[2])];
+                            continue;
+                        }
+                        const Real gh = ghost(0, s, sol, in[0], in[1], in[2], true);
+                        const Real xin = sol[idx(g, in[0], in[1], in[2])];
+                        F(i, j, k) = lo ? (xin - gh) * dxi : (gh - xin) * dxi;
+                    }
+        }
+    }
+};
+
+} // namespace
+
+// ---------------------------------------------------------------- context
+struct OCtx
+{
+    vd_config cfg;
+    Geom geo;
+    ProbParm pp;
+    Fab phi_new, phi_old;
+    double cur_time = 0.0;
+    int istep = 0;
+    int ngrow = 3;
+    int E_IDX = E_ID;
+    std::vector<int> bg;
+    std::string err;
+    long long n_poisson_iters = 0, n_species_iters = 0;
+};
+
+namespace {
+
+GpuArray<Real, 3> ga(const Real* v) { return GpuArray<Real, 3>{{v[0], v[1], v[2]}}; }
+
+bool is_bg(const OCtx& c, int sp)
+{
+    return std::find(c.bg.begin(), c.bg.end(), sp) != c.bg.end();
+}
+
+// Boundary data of one solve (per side: value, robin a/b/f), filled by the
+// case callbacks exactly where the reference's hooks write ghost cells.
+struct BndryData
+{
+    std::vector<Real> val[6], ra[6], rb[6], rf[6];
+};
+
+void set_bc_types(OMG& mg, const Geom& geo, const int* lo, const int* hi)
+{
+    for (int d = 0; d < 3; ++d)
+    {
+        if (d >= geo.dim || geo.per[d])
+        {
+            mg.type[d] = O_PER;
+            mg.type[d + 3] = O_PER;
+            continue;
+        }
+        mg.type[d] = map_bc(lo[d]);
+        mg.type[d + 3] = map_bc(hi[d]);
+    }
+}
+
+// Views over one boundary side: an Array4 whose box is the ghost layer.
+Array4 side_view(std::vector<Real>& v, const Geom& g, int s)
+{
+    const int d = s % 3;
+    Array4 a;
+    a.p = v.data();
+    for (int q = 0; q < 3; ++q)
+    {
+        a.lo[q] = 0;
+        a.hi[q] = g.n[q] - 1;
+    }
+    a.lo[d] = a.hi[d] = (s / 3) ? g.n[d] : -1;
+    a.jstride = a.hi[0] - a.lo[0] + 1;
+    a.kstride = a.jstride * (a.hi[1] - a.lo[1] + 1);
+    a.nstride = a.kstride * (a.hi[2] - a.lo[2] + 1);
+    return a;
+}
+
+Real applied_potential(Real t, int domend, int vprof, Real v1, Real v2,
+                       Real vfreq, Real vdur, Real vcen)
+{
+    // Source/HelperFuncs.H:125-161
+    const Real amp = (domend == -1) ? v1 : v2;
+    if (vprof == 1) return std::sin(2.0 * PI * vfreq * t) * amp;
+    if (vprof == 2)
+    {
+        if (t <= vcen)
+            return (vcen - t < vdur / 2.0) ? (1.0 - (vcen - t) / (vdur / 2.0)) * amp : 0.0;
+        return (t - vcen < vdur / 2.0) ? (1.0 - (t - vcen) / (vdur / 2.0)) * amp : 0.0;
+    }
+    return amp;
+}
+
+// --- solve_potential (Source/PotentialSolve.cpp:19-554) ----------------
+void solve_potential(OCtx& c, Real time, Fab& Sborder, Fab& Sborder_old,
+                     FaceFab* efield_fc, vd_solve_stats* st)
+{
+    const Geom& geo = c.geo;
+    const vd_config& cfg = c.cfg;
+    OMG mg;
+    mg.dim = geo.dim;
+    mg.maxorder = 2;
+    mg.alpha = 1.0 * 0.0;
+    mg.beta = 1.0;
+    mg.nu1 = cfg.linsolve_num_pre_smooth;
+    mg.nu2 = cfg.linsolve_num_post_smooth;
+    mg.maxiter = cfg.linsolve_maxiter;
+    mg.build(geo, cfg.linsolve_max_coarsening_level);
+    set_bc_types(mg, geo, cfg.pot_bc_lo, cfg.pot_bc_hi);
+    const long long N = geo.ncell();
+
+    std::vector<Real> rhs(N, 0.0), sol(N, 0.0);
+    Array4 sbo = Sborder_old.view();
+    Array4 sb = Sborder.view();
+    const auto dx = ga(geo.dx), plo = ga(geo.lo), phi_ = ga(geo.hi);
+    if (cfg.do_spacechrg)
+    {
+#pragma omp parallel for collapse(2)
+        for (int k = 0; k < geo.n[2]; ++k)
+            for (int j = 0; j < geo.n[1]; ++j)
+                for (int i = 0; i < geo.n[0]; ++i)
+                {
+                    Real r = 0.0;
+                    for (int sp = 0; sp < NUM_SPECIES; sp++)
+                        if (std::abs(plasmachem::get_charge(sp)) > 0)
+                            r += plasmachem::get_charge(sp) * sbo(i, j, k, sp);
+                    r *= (-ECHARGE / EPS0);
+                    Fab tmp;
+                    Array4 rv;
+                    rv.p = &r;
+                    rv.lo[0] = i; rv.lo[1] = j; rv.lo[2] = k;
+                    rv.hi[0] = i; rv.hi[1] = j; rv.hi[2] = k;
+                    rv.jstride = rv.kstride = rv.nstride = 1;
+                    user_sources::add_user_potential_sources(i, j, k, sbo, rv, plo, phi_, dx, time, c.pp);
+                    rhs[OMG::idx(geo, i, j, k)] = r;
+                }
+    }
+    // coefficients: a = 0, b = -1 harmonic-averaged (= -1)
+    for (int d = 0; d < 3; ++d) std::fill(mg.L[0].b[d].begin(), mg.L[0].b[d].end(), -1.0);
+    // boundary data via potential_bc
+    BndryData bd;
+    for (int s = 0; s < 6; ++s)
+    {
+        const int d = s % 3;
+        const int np = OMG::plane_size(geo, d);
+        bd.val[s].assign(np, 0.0);
+        bd.ra[s].assign(np, 0.0);
+        bd.rb[s].assign(np, 1.0);
+        bd.rf[s].assign(np, 0.0);
+        if (d >= geo.dim || geo.per[d]) continue;
+        // `potential` holds Sborder's POT (ghosts by foextrap) before the hook
+        for (int q = 0; q < np; ++q)
+        {
+            int ta = (d == 0) ? 1 : 0, tb = (d == 2) ? 1 : 2;
+            int cc[3];
+            cc[d] = (s / 3) ? geo.n[d] - 1 : 0;
+            cc[ta] = q % geo.n[ta];
+            cc[tb] = q / geo.n[ta];
+            bd.val[s][q] = sb(cc[0], cc[1], cc[2], POT_ID);
+        }
+        Array4 bv = side_view(bd.val[s], geo, s), av = side_view(bd.ra[s], geo, s),
+               bbv = side_view(bd.rb[s], geo, s), fv = side_view(bd.rf[s], geo, s);
+        const int sgn = (s / 3) ? 1 : -1;
+        const Real app = applied_potential(time, sgn, cfg.voltage_profile,
+                                           cfg.voltage_amp_lo[d], cfg.voltage_amp_hi[d],
+                                           cfg.voltage_freq, cfg.voltage_dur, cfg.voltage_center);
+        for (int q = 0; q < np; ++q)
+        {
+            int ta = (d == 0) ? 1 : 0, tb = (d == 2) ? 1 : 2;
+            int f[3];
+            f[d] = (s / 3) ? geo.n[d] : 0;
+            f[ta] = q % geo.n[ta];
+            f[tb] = q / geo.n[ta];
+#ifdef VD_HAS_USER_TRANSPORT
+            if (cfg.user_defined_potential)
+                user_transport::potential_bc(f[0], f[1], f[2], d, sgn, sb, bv, av, bbv, fv,
+                                             plo, phi_, dx, time, c.pp, cfg.gas_temperature,
+                                             cfg.gas_pressure, app);
+            else
+#endif
+                plasmachem_transport::potential_bc(f[0], f[1], f[2], d, sgn, sb, bv, av, bbv,
+                                                   fv, plo, phi_, dx, time, c.pp,
+                                                   cfg.gas_temperature, cfg.gas_pressure, app);
+        }
+    }
+    const Real ps = cfg.potential_scale;
+    for (int s = 0; s < 6; ++s)
+    {
+        for (auto& v : bd.val[s]) v *= 1.0 / ps;
+        for (auto& v : bd.rf[s]) v *= 1.0 / ps;
+        mg.bval[s] = bd.val[s];
+        mg.rf[s] = bd.rf[s];
+        mg.L[0].ra[s] = bd.ra[s];
+        mg.L[0].rb[s] = bd.rb[s];
+    }
+    mg.average_down_coeffs();
+    for (auto& v : rhs) v *= 1.0 / ps;
+    if (cfg.poisson_warm_start)
+        for (int k = 0; k < geo.n[2]; ++k)
+            for (int j = 0; j < geo.n[1]; ++j)
+                for (int i = 0; i < geo.n[0]; ++i)
+                    sol[OMG::idx(geo, i, j, k)] = sb(i, j, k, POT_ID) / ps;
+    const int it = mg.solve(sol, rhs, cfg.linsolve_reltol, cfg.linsolve_abstol, st);
+    if (it > 0) c.n_poisson_iters += it;
+    if (it < 0) c.n_poisson_iters += cfg.linsolve_maxiter;
+
+    mg.grad(sol, efield_fc);
+    for (int d = 0; d < geo.dim; ++d)
+        for (auto& v : efield_fc[d].d) v *= -1.0 * ps;
+    // face -> cell average, reduced field, potential
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k < geo.n[2]; ++k)
+        for (int j = 0; j < geo.n[1]; ++j)
+            for (int i = 0; i < geo.n[0]; ++i)
+            {
+                Real E[3] = {0, 0, 0};
+                for (int d = 0; d < geo.dim; ++d)
+                {
+                    int p[3] = {i, j, k};
+                    p[d] += 1;
+                    E[d] = 0.5 * (efield_fc[d](i, j, k) + efield_fc[d](p[0], p[1], p[2]));
+                    c.phi_new(i, j, k, EFX_ID + d) = E[d];
+                }
+                Real Esum = 0.0, nd = 0.0;
+                for (int sp = 0; sp < NUM_SPECIES; sp++) nd += c.phi_new(i, j, k, sp);
+                nd = nd - c.phi_new(i, j, k, E_ID);
+                for (int d = 0; d < geo.dim; ++d) Esum += E[d] * E[d];
+                c.phi_new(i, j, k, REF_ID) = (std::pow(Esum, 0.5) / nd) / 1.0e-21;
+                c.phi_new(i, j, k, POT_ID) = sol[OMG::idx(geo, i, j, k)] * ps;
+            }
+}
+
+// --- update_rxnsrc_at_all_levels (Source/ScalarSolve.cpp:156-216) -------
+void update_rxnsrc(OCtx& c, Fab& Sborder, Fab& rxn, Real time)
+{
+    const Geom& geo = c.geo;
+    rxn.setVal(0.0);
+    if (!c.cfg.do_reactions) return;
+    Array4 sb = Sborder.view();
+    Array4 rv = rxn.view();
+    const auto dx = ga(geo.dx), plo = ga(geo.lo), phi_ = ga(geo.hi);
+    const Real Tg = c.cfg.gas_temperature, Pg = c.cfg.gas_pressure;
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k < geo.n[2]; ++k)
+        for (int j = 0; j < geo.n[1]; ++j)
+            for (int i = 0; i < geo.n[0]; ++i)
+            {
+                Real C[NUM_SPECIES], W[NUM_SPECIES];
+                const Real Te = sb(i, j, k, ETEMP_ID), EN = sb(i, j, k, REF_ID);
+                Real ee = 0.0;
+                for (int sp = 0; sp < NUM_SPECIES; sp++) C[sp] = sb(i, j, k, sp) / N_A;
+                CKWC(Tg, C, W, Te, EN, &ee);
+                for (int sp = 0; sp < NUM_SPECIES; sp++) rv(i, j, k, sp) = W[sp] * N_A;
+                rv(i, j, k, NUM_SPECIES) = ee;
+                user_sources::add_user_react_sources(i, j, k, sb, rv, plo, phi_, dx, time, c.pp, Tg, Pg);
+            }
+}
+
+// --- compute_flux (Source/compute_explicit_flux.H:218-415) --------------
+Real vel_at(OCtx& c, Array4 const& sb, IntVect cell, int dir, int sp, Real time)
+{
+    const auto dx = ga(c.geo.dx);
+#ifdef VD_HAS_USER_TRANSPORT
+    if (c.cfg.user_defined_vel)
+        return user_transport::compute_vel(cell, dir, sp, sb, dx, time, c.pp,
+                                           c.cfg.gas_temperature, c.cfg.gas_pressure);
+#endif
+    return plasmachem_transport::compute_vel(cell, dir, sp, sb, dx, time, c.pp,
+                                             c.cfg.gas_temperature, c.cfg.gas_pressure);
+}
+
+Real face_flux(OCtx& c, Array4 const& sb, int i, int j, int k, int dir, int sp,
+               const int* bclo, const int* bchi, Real time)
+{
+    IntVect face{i, j, k}, left{i, j, k}, right{i, j, k};
+    left[dir] -= 1;
+    const Real pL = sb(left, sp), pR = sb(right, sp);
+    Real fx = 0.0;
+    const Real vL = vel_at(c, sb, left, dir, sp, time);
+    const Real vR = vel_at(c, sb, right, dir, sp, time);
+    const int ho = c.cfg.hyp_order;
+    if (ho == 1)
+        fx = o_upwind(vL, vR, pL, pR);
+    else if (ho == 2)
+    {
+        IntVect l1 = face, r1 = face;
+        l1[dir] -= 2;
+        r1[dir] += 1;
+        Real dxmin = c.geo.dx[0];
+        for (int d = 1; d < c.geo.dim; ++d) dxmin = std::min(dxmin, c.geo.dx[d]);
+        fx = o_waf(vL, vR, sb(l1, sp), pL, pR, sb(r1, sp), dxmin, c.cfg.dt);
+    } else
+    {
+        IntVect l1 = face, r1 = face, l2 = face, r2 = face;
+        l1[dir] -= 2;
+        r1[dir] += 1;
+        l2[dir] -= 3;
+        r2[dir] += 2;
+        const Real vLm1 = vel_at(c, sb, l1, dir, sp, time);
+        const Real vLm2 = vel_at(c, sb, l2, dir, sp, time);
+        const Real vRp1 = vel_at(c, sb, r1, dir, sp, time);
+        const Real vRp2 = vel_at(c, sb, r2, dir, sp, time);
+        const Real ulm2 = sb(l2, sp), ulm1 = sb(l1, sp), ul = pL, ur = pR,
+                   urp1 = sb(r1, sp), urp2 = sb(r2, sp);
+        const Real flm2 = ulm2 * vLm2, flm1 = ulm1 * vLm1, fl = ul * vL,
+                   fr = ur * vR, frp1 = urp1 * vRp1, frp2 = urp2 * vRp2;
+        const Real lam = std::fabs(0.5 * (vL + vR));
+        const int ws = c.cfg.weno_scheme;
+        const Real fph = o_weno(flm2, flm1, fl, fr, frp1, ws);
+        const Real fmh = o_weno(frp2, frp1, fr, fl, flm1, ws);
+        const Real uph = o_weno(ulm2, ulm1, ul, ur, urp1, ws);
+        const Real umh = o_weno(urp2, urp1, ur, ul, ulm1, ws);
+        fx = 0.5 * (fph + lam * uph) + 0.5 * (fmh - lam * umh);
+    }
+    if (face[dir] == 0 && (bclo[dir] == IHNEUBC || bclo[dir] == AXISBC)) fx = 0.0;
+    if (face[dir] == c.geo.n[dir] && (bchi[dir] == IHNEUBC || bchi[dir] == AXISBC)) fx = 0.0;
+    return fx;
+}
+
+// --- update_explsrc_at_all_levels + compute_dsdt ---------------------------
+void update_explsrc(OCtx& c, int sp, const int* bclo, const int* bchi,
+                    Fab& Sborder, Fab& rxn, Fab& expl, Real time)
+{
+    const Geom& geo = c.geo;
+    Array4 sb = Sborder.view();
+    FaceFab flux[3];
+    for (int d = 0; d < geo.dim; ++d)
+    {
+        flux[d].define(geo, d, 1);
+        if (!c.cfg.do_transport) continue;
+        FaceFab& F = flux[d];
+#pragma omp parallel for collapse(2)
+        for (int k = 0; k < F.n[2]; ++k)
+            for (int j = 0; j < F.n[1]; ++j)
+                for (int i = 0; i < F.n[0]; ++i)
+                    F(i, j, k) = face_flux(c, sb, i, j, k, d, sp, bclo, bchi, time);
+    }
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k < geo.n[2]; ++k)
+        for (int j = 0; j < geo.n[1]; ++j)
+            for (int i = 0; i < geo.n[0]; ++i)
+            {
+                Real v = (flux[0](i, j, k) - flux[0](i + 1, j, k)) / geo.dx[0] + rxn(i, j, k, sp);
+                if (geo.dim > 1) v += (flux[1](i, j, k) - flux[1](i, j + 1, k)) / geo.dx[1];
+                if (geo.dim > 2) v += (flux[2](i, j, k) - flux[2](i, j, k + 1)) / geo.dx[2];
+                expl(i, j, k, sp) = v;
+            }
+}
+
+// --- get_onesided_grad (Source/HelperFuncs.H:13-52) ----------------------
+Real onesided_grad(IntVect face, int sgn, int idim, int comp, const Real* dx,
+                   Array4 const& sb)
+{
+    IntVect cell = face;
+    cell[idim] += (sgn == 1) ? -1 : 0;
+    IntVect n1 = cell, n2 = cell;
+    n1[idim] = cell[idim] - sgn;
+    n2[idim] = n1[idim] - sgn;
+    Real g1, g2;
+    if (sgn == -1)
+    {
+        g1 = (sb(n1, comp) - sb(cell, comp)) / dx[idim];
+        g2 = (sb(n2, comp) - sb(n1, comp)) / dx[idim];
+    } else
+    {
+        g1 = (sb(cell, comp) - sb(n1, comp)) / dx[idim];
+        g2 = (sb(n1, comp) - sb(n2, comp)) / dx[idim];
+    }
+    return 2.0 * g1 - g2;
+}
+
+// --- compute_elecenergy_source (Source/ElecEnergySource.cpp:72-294) -----
+void elecenergy_source(OCtx& c, Fab& Sborder, Fab& rxn, FaceFab* efield,
+                       FaceFab* gradne, Fab& expl)
+{
+    const Geom& geo = c.geo;
+    Array4 sb = Sborder.view();
+    const int eidx = c.E_IDX;
+    const Real Tg = c.cfg.gas_temperature;
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k < geo.n[2]; ++k)
+        for (int j = 0; j < geo.n[1]; ++j)
+            for (int i = 0; i < geo.n[0]; ++i)
+            {
+                const Real charge = plasmachem::get_charge(eidx) * ECHARGE;
+                Real jh = 0.0;
+                for (int d = 0; d < geo.dim; ++d)
+                    for (int f = 0; f < 2; ++f)
+                    {
+                        IntVect face{i, j, k};
+                        face[d] += f;
+                        IntVect lc = face, rc = face;
+                        lc[d] -= 1;
+                        const Real te = (sb(lc, ETEMP_ID) + sb(rc, ETEMP_ID)) / 2.0;
+                        Real Esum = 0.0;
+                        for (int q = 0; q < geo.dim; ++q)
+                        {
+                            const Real e = (sb(lc, EFX_ID + q) + sb(rc, EFX_ID + q)) / 2.0;
+                            Esum += e * e;
+                        }
+                        const Real emag = std::sqrt(Esum);
+                        const Real ne = (sb(lc, eidx) + sb(rc, eidx)) / 2.0;
+                        const Real ef = efield[d](face[0], face[1], face[2]);
+                        Real nd = 0.0;
+                        for (int sp = 0; sp < NUM_SPECIES; sp++)
+                            nd += (sb(lc, sp) + sb(rc, sp)) / 2.0;
+                        const Real mu = specMob(eidx, te, nd, emag, Tg);
+                        const Real dc = specDiff(eidx, te, nd, emag, Tg);
+                        Real gn;
+                        if (face[d] == 0 || face[d] == geo.n[d])
+                        {
+                            const int sgn = (face[d] == 0) ? -1 : 1;
+                            gn = onesided_grad(face, sgn, d, eidx, geo.dx, sb);
+                        } else
+                            gn = gradne[d](face[0], face[1], face[2]);
+                        const Real cd = charge * (mu * ne * ef - dc * gn);
+                        jh += cd * ef;
+                    }
+                jh *= 0.5;
+                if (c.cfg.floor_jh && jh < 0.0) jh = 0.0;
+                expl(i, j, k, NUM_SPECIES) += jh;
+                c.phi_new(i, j, k, EJH_ID) = jh;
+                c.phi_new(i, j, k, EIH_ID) = rxn(i, j, k, EEN_ID);
+            }
+}
+
+// --- implicit_solve_scalar (Source/ScalarSolve.cpp:380-1000) -------------
+void implicit_solve(OCtx& c, Real time, Real dt, int spec, Fab& Sborder,
+                    Fab& Sborder_old, Fab& expl, const int* bclo, const int* bchi,
+                    FaceFab* grad_out, vd_solve_stats* st)
+{
+    const Geom& geo = c.geo;
+    const vd_config& cfg = c.cfg;
+    const bool is_e = (spec == c.E_IDX);
+    const bool is_een = (spec == EEN_ID);
+    const Real ts = cfg.time_scale;
+    const Real scale = is_een ? cfg.elecenergy_scale : cfg.species_scale[spec];
+    OMG mg;
+    mg.dim = geo.dim;
+    mg.maxorder = 3;
+    mg.alpha = 1.0;
+    mg.beta = ts;
+    mg.nu1 = cfg.linsolve_num_pre_smooth;
+    mg.nu2 = cfg.linsolve_num_post_smooth;
+    mg.maxiter = cfg.linsolve_maxiter;
+    mg.build(geo, cfg.linsolve_max_coarsening_level);
+    set_bc_types(mg, geo, bclo, bchi);
+    const long long N = geo.ncell();
+    Array4 sb = Sborder.view();
+    Array4 sbo = Sborder_old.view();
+    const Real Tg = cfg.gas_temperature, Pg = cfg.gas_pressure;
+
+    std::vector<Real> rhs(N), sol(N);
+    // acoeff = 1/dt * timescale; rhs = (1/dt) n_old + S_expl, scaled
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k < geo.n[2]; ++k)
+        for (int j = 0; j < geo.n[1]; ++j)
+            for (int i = 0; i < geo.n[0]; ++i)
+            {
+                const long long p = OMG::idx(geo, i, j, k);
+                mg.L[0].a[p] = (1.0 / dt) * ts;
+                Real r = (1.0 / dt) * sbo(i, j, k, spec) + 1.0 * expl(i, j, k, spec);
+                rhs[p] = r * (ts / scale);
+                sol[p] = sb(i, j, k, spec) * (1.0 / scale);
+            }
+    // cell D on the grown box, harmonic face average (boundary faces use the
+    // foextrap ghost, i.e. the boundary cell itself)
+    auto Dcell = [&](int i, int j, int k) {
+        Real Es = 0.0, nd = 0.0;
+        for (int d = 0; d < 3; ++d) Es += sb(i, j, k, EFX_ID + d) * sb(i, j, k, EFX_ID + d);
+        const Real emag = std::sqrt(Es);
+        for (int sp = 0; sp < NUM_SPECIES; sp++) nd += sb(i, j, k, sp);
+        return specDiff(spec, sb(i, j, k, ETEMP_ID), nd, emag, Tg);
+    };
+    for (int d = 0; d < geo.dim; ++d)
+    {
+        const int nx = geo.n[0] + (d == 0), ny = geo.n[1] + (d == 1), nz = geo.n[2] + (d == 2);
+#pragma omp parallel for collapse(2)
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i)
+                {
+                    int m[3] = {i, j, k};
+                    m[d] -= 1;
+                    const Real d0 = Dcell(m[0], m[1], m[2]), d1 = Dcell(i, j, k);
+                    const Real den = d0 + d1;
+                    mg.L[0].b[d][OMG::fidx(geo, d, i, j, k)] =
+                        (den != 0.0) ? 2.0 * d0 * d1 / den : 0.0;
+                }
+    }
+    // boundary data via species_bc; `specdata` ghosts start as Sborder's
+    BndryData bd;
+    const auto dx = ga(geo.dx), plo = ga(geo.lo), phi_ = ga(geo.hi);
+    for (int s = 0; s < 6; ++s)
+    {
+        const int d = s % 3;
+        const int np = OMG::plane_size(geo, d);
+        bd.val[s].assign(np, 0.0);
+        bd.ra[s].assign(np, 0.0);
+        bd.rb[s].assign(np, 1.0);
+        bd.rf[s].assign(np, 0.0);
+        if (d >= geo.dim || geo.per[d]) continue;
+        const int ta = (d == 0) ? 1 : 0, tb = (d == 2) ? 1 : 2;
+        for (int q = 0; q < np; ++q)
+        {
+            int cc[3];
+            cc[d] = (s / 3) ? geo.n[d] - 1 : 0;
+            cc[ta] = q % geo.n[ta];
+            cc[tb] = q / geo.n[ta];
+            bd.val[s][q] = sb(cc[0], cc[1], cc[2], spec);
+        }
+        Array4 bv = side_view(bd.val[s], geo, s), av = side_view(bd.ra[s], geo, s),
+               bbv = side_view(bd.rb[s], geo, s), fv = side_view(bd.rf[s], geo, s);
+        const int sgn = (s / 3) ? 1 : -1;
+        for (int q = 0; q < np; ++q)
+        {
+            int f[3];
+            f[d] = (s / 3) ? geo.n[d] : 0;
+            f[ta] = q % geo.n[ta];
+            f[tb] = q / geo.n[ta];
+#ifdef VD_HAS_USER_TRANSPORT
+            if (cfg.user_defined_species)
+                user_transport::species_bc(f[0], f[1], f[2], d, sgn, spec, 0, sb, bv, av, bbv, fv,
+                                           plo, phi_, dx, time, c.pp, Tg, Pg);
+            else
+#endif
+                plasmachem_transport::species_bc(f[0], f[1], f[2], d, sgn, spec, 0, sb, bv, av,
+                                                 bbv, fv, plo, phi_, dx, time, c.pp, Tg, Pg);
+        }
+    }
+    for (int s = 0; s < 6; ++s)
+    {
+        for (auto& v : bd.val[s]) v *= 1.0 / scale;
+        for (auto& v : bd.rf[s]) v *= 1.0 / scale;
+        mg.bval[s] = bd.val[s];
+        mg.rf[s] = bd.rf[s];
+        mg.L[0].ra[s] = bd.ra[s];
+        mg.L[0].rb[s] = bd.rb[s];
+    }
+    mg.average_down_coeffs();
+    const int it = mg.solve(sol, rhs, cfg.linsolve_reltol, cfg.linsolve_abstol, st);
+    if (it > 0) c.n_species_iters += it;
+    if (it < 0) c.n_species_iters += cfg.linsolve_maxiter;
+    if (is_e && grad_out)
+    {
+        mg.grad(sol, grad_out);
+        for (int d = 0; d < geo.dim; ++d)
+            for (auto& v : grad_out[d].d) v *= cfg.species_scale[c.E_IDX];
+    }
+    // scale back, floor, copy into phi_new
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k < geo.n[2]; ++k)
+        for (int j = 0; j < geo.n[1]; ++j)
+            for (int i = 0; i < geo.n[0]; ++i)
+            {
+                Real v = sol[OMG::idx(geo, i, j, k)] * scale;
+                if (cfg.bound_specden && !is_een)
+                {
+                    if (is_e)
+                    {
+                        if (v < cfg.min_electron_density) v = cfg.min_electron_density;
+                    } else if (v < cfg.min_species_density)
+                        v = cfg.min_species_density;
+                }
+                c.phi_new(i, j, k, spec) = v;
+            }
+    if (is_een)
+    {
+        const Real minT = cfg.min_electron_temp;
+#pragma omp parallel for collapse(2)
+        for (int k = 0; k < geo.n[2]; ++k)
+            for (int j = 0; j < geo.n[1]; ++j)
+                for (int i = 0; i < geo.n[0]; ++i)
+                {
+                    Real te = twothird / K_B * c.phi_new(i, j, k, EEN_ID) / sb(i, j, k, c.E_IDX);
+                    c.phi_new(i, j, k, ETEMP_ID) = te;
+                    if (te < minT)
+                    {
+                        c.phi_new(i, j, k, ETEMP_ID) = minT;
+                        c.phi_new(i, j, k, EEN_ID) = 1.5 * K_B * c.phi_new(i, j, k, c.E_IDX) * minT;
+                    }
+                }
+    }
+}
+
+// --- compute_electemp_lfa (Source/ElecEnergySource.cpp:17-70) ------------
+void electemp_lfa(OCtx& c, Fab& Sborder)
+{
+    const Geom& geo = c.geo;
+    Array4 sb = Sborder.view();
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k < geo.n[2]; ++k)
+        for (int j = 0; j < geo.n[1]; ++j)
+            for (int i = 0; i < geo.n[0]; ++i)
+            {
+                if (!int(sb(i, j, k, CMASK_ID))) continue;
+                Real spec[NUM_SPECIES];
+                for (int sp = 0; sp < NUM_SPECIES; sp++) spec[sp] = sb(i, j, k, sp);
+                Real te = etempLFA(c.cfg.gas_temperature, spec, sb(i, j, k, REF_ID));
+                if (te < c.cfg.min_electron_temp) te = c.cfg.min_electron_temp;
+                c.phi_new(i, j, k, ETEMP_ID) = te;
+                c.phi_new(i, j, k, EEN_ID) =
+                    1.5 * K_B * c.phi_new(i, j, k, c.E_IDX) * c.cfg.min_electron_temp;
+            }
+}
+
+const int* bc_lo_for(const OCtx& c, int sp)
+{
+    if (sp == c.E_IDX) return c.cfg.eden_bc_lo;
+    if (sp == EEN_ID) return c.cfg.eenrg_bc_lo;
+    return plasmachem::get_charge(sp) != 0 ? c.cfg.ion_bc_lo : c.cfg.neutral_bc_lo;
+}
+const int* bc_hi_for(const OCtx& c, int sp)
+{
+    if (sp == c.E_IDX) return c.cfg.eden_bc_hi;
+    if (sp == EEN_ID) return c.cfg.eenrg_bc_hi;
+    return plasmachem::get_charge(sp) != 0 ? c.cfg.ion_bc_hi : c.cfg.neutral_bc_hi;
+}
+
+// --- one coarse step (Source/Evolve.cpp:136-617) -------------------------
+void evolve_one(OCtx& c)
+{
+    const Geom& geo = c.geo;
+    const Real dt = c.cfg.dt;
+    c.phi_old.d = c.phi_new.d; // copy new -> old
+    Fab Sborder, Sborder_old, rxn, expl;
+    Sborder.define(geo, NVAR, c.ngrow);
+    Sborder_old.define(geo, NVAR, c.ngrow);
+    rxn.define(geo, NUM_SPECIES + 1, 0);
+    expl.define(geo, NUM_SPECIES + 1, 0);
+    fill_patch(geo, c.phi_old, Sborder_old, NVAR);
+    FaceFab efield[3], gradne[3];
+    for (int d = 0; d < 3; ++d)
+    {
+        efield[d].define(geo, d, 1);
+        gradne[d].define(geo, d, 1);
+    }
+    const int ncorr = c.cfg.num_timestep_correctors;
+    for (int niter = 0; niter < ncorr; ++niter)
+    {
+        const Real toff = (niter > 0) ? 0.5 * dt : 0.0;
+        const Real t = c.cur_time + toff;
+        fill_patch(geo, c.phi_new, Sborder, NVAR);
+        expl.setVal(0.0);
+        solve_potential(c, t, Sborder, Sborder_old, efield, nullptr);
+        fill_patch(geo, c.phi_new, Sborder, NVAR);
+        rxn.setVal(0.0);
+        if (c.cfg.do_reactions) update_rxnsrc(c, Sborder, rxn, t);
+        const int e = c.E_IDX;
+        expl.setVal(0.0);
+        update_explsrc(c, e, c.cfg.eden_bc_lo, c.cfg.eden_bc_hi, Sborder, rxn, expl, t);
+        implicit_solve(c, t, dt, e, Sborder, Sborder_old, expl, c.cfg.eden_bc_lo,
+                       c.cfg.eden_bc_hi, gradne, nullptr);
+        if (c.cfg.elecenergy_solve)
+        {
+            expl.setVal(0.0);
+            update_explsrc(c, EEN_ID, c.cfg.eenrg_bc_lo, c.cfg.eenrg_bc_hi, Sborder, rxn, expl, t);
+            elecenergy_source(c, Sborder, rxn, efield, gradne, expl);
+            implicit_solve(c, t, dt, EEN_ID, Sborder, Sborder_old, expl, c.cfg.eenrg_bc_lo,
+                           c.cfg.eenrg_bc_hi, nullptr, nullptr);
+        }
+        if (c.cfg.using_LFA) electemp_lfa(c, Sborder);
+        for (int sp = 0; sp < NUM_SPECIES; ++sp)
+        {
+            const bool bgs = is_bg(c, sp);
+            if (!(bgs || sp == e))
+            {
+                expl.setVal(0.0);
+                update_explsrc(c, sp, bc_lo_for(c, sp), bc_hi_for(c, sp), Sborder, rxn, expl, t);
+                implicit_solve(c, t, dt, sp, Sborder, Sborder_old, expl, bc_lo_for(c, sp),
+                               bc_hi_for(c, sp), nullptr, nullptr);
+            }
+            if (bgs && c.cfg.do_bg_reactions)
+            {
+                for (int k = 0; k < geo.n[2]; ++k)
+                    for (int j = 0; j < geo.n[1]; ++j)
+                        for (int i = 0; i < geo.n[0]; ++i)
+                        {
+                            Real& v = c.phi_new(i, j, k, sp);
+                            v += rxn(i, j, k, sp) * dt;
+                            if (v < c.cfg.min_species_density && c.cfg.bound_specden)
+                                v = c.cfg.min_species_density;
+                        }
+            }
+        }
+        if (niter < ncorr - 1)
+        {
+            for (size_t q = 0; q < c.phi_new.d.size(); ++q)
+                c.phi_new.d[q] = 0.5 * c.phi_old.d[q] + 0.5 * c.phi_new.d[q];
+        }
+    }
+    c.cur_time += dt;
+    c.istep += 1;
+}
+
+Geom geom_of(const vd_config& cfg)
+{
+    Geom g;
+    g.dim = cfg.dim;
+    for (int d = 0; d < 3; ++d)
+    {
+        if (d < cfg.dim)
+        {
+            g.n[d] = cfg.n_cell[d];
+            g.lo[d] = cfg.prob_lo[d];
+            g.hi[d] = cfg.prob_hi[d];
+            g.dx[d] = (g.hi[d] - g.lo[d]) / g.n[d];
+            g.per[d] = cfg.is_periodic[d];
+        } else
+        {
+            g.n[d] = 1;
+            g.lo[d] = 0.0;
+            g.hi[d] = 1.0;
+            g.dx[d] = 1.0;
+            g.per[d] = 0;
+        }
+    }
+    return g;
+}
+
+} // namespace
+
+// ================================================================ C entry
+extern "C" {
+
+int vdo_create(const vd_config* cfg, void** out)
+{
+    if (!cfg || !out) return VD_ERR_INVALID_ARG;
+    auto* c = new OCtx();
+    c->cfg = *cfg;
+    c->geo = geom_of(*cfg);
+    c->ngrow = (cfg->hyp_order == 1) ? 1 : (cfg->hyp_order == 2 ? 2 : 3);
+    c->phi_new.define(c->geo, NVAR, 0);
+    c->phi_old.define(c->geo, NVAR, 0);
+    for (int i = 0; i < cfg->num_bg_species; ++i) c->bg.push_back(cfg->bg_species_ids[i]);
+    *out = c;
+    return VD_OK;
+}
+
+int vdo_destroy(void* ctx)
+{
+    delete static_cast<OCtx*>(ctx);
+    return VD_OK;
+}
+
+int vdo_init_domain(void* ctx, const char* text)
+{
+    auto* c = static_cast<OCtx*>(ctx);
+    auto table = vd::ParmParse::parse(text ? text : "");
+    vd::ParmParse pp(&table, "prob");
+    c->pp = ProbParm{};
+    amrex_probinit(c->pp, pp);
+    vd::GeometryData gd;
+    for (int d = 0; d < 3; ++d)
+    {
+        gd.prob_lo[d] = c->geo.lo[d];
+        gd.prob_hi[d] = c->geo.hi[d];
+        gd.dx[d] = c->geo.dx[d];
+        gd.n_cell[d] = c->geo.n[d];
+    }
+    vd::Box bx{{0, 0, 0}, {c->geo.n[0] - 1, c->geo.n[1] - 1, c->geo.n[2] - 1}};
+    Array4 v = c->phi_new.view();
+    initdomaindata(bx, v, gd, &c->pp);
+    c->phi_old.d = c->phi_new.d;
+    c->cur_time = 0.0;
+    c->istep = 0;
+    return VD_OK;
+}
+
+int vdo_set_probinit(void* ctx, const char* text)
+{
+    auto* c = static_cast<OCtx*>(ctx);
+    auto table = vd::ParmParse::parse(text ? text : "");
+    vd::ParmParse pp(&table, "prob");
+    c->pp = ProbParm{};
+    amrex_probinit(c->pp, pp);
+    return VD_OK;
+}
+
+int vdo_set_state(void* ctx, int comp, int ncomp, const double* src)
+{
+    auto* c = static_cast<OCtx*>(ctx);
+    const long long N = c->geo.ncell();
+    std::memcpy(c->phi_new.d.data() + (size_t)comp * N, src, sizeof(double) * N * ncomp);
+    return VD_OK;
+}
+
+int vdo_get_state(void* ctx, int comp, int ncomp, double* dst)
+{
+    auto* c = static_cast<OCtx*>(ctx);
+    const long long N = c->geo.ncell();
+    std::memcpy(dst, c->phi_new.d.data() + (size_t)comp * N, sizeof(double) * N * ncomp);
+    return VD_OK;
+}
+
+int vdo_set_time(void* ctx, double t, int step)
+{
+    auto* c = static_cast<OCtx*>(ctx);
+    c->cur_time = t;
+    c->istep = step;
+    return VD_OK;
+}
+
+int vdo_step(void* ctx, int nsteps, vd_step_stats* st)
+{
+    auto* c = static_cast<OCtx*>(ctx);
+    c->n_poisson_iters = 0;
+    c->n_species_iters = 0;
+    for (int s = 0; s < nsteps; ++s) evolve_one(*c);
+    if (st)
+    {
+        std::memset(st, 0, sizeof(*st));
+        st->steps = nsteps;
+        st->poisson_iterations = (int)c->n_poisson_iters;
+        st->species_iterations = (int)c->n_species_iters;
+        st->time = c->cur_time;
+    }
+    return VD_OK;
+}
+
+int vdo_poisson_solve(void* ctx, double time, vd_solve_stats* st)
+{
+    auto* c = static_cast<OCtx*>(ctx);
+    Fab Sb;
+    Sb.define(c->geo, NVAR, c->ngrow);
+    fill_patch(c->geo, c->phi_new, Sb, NVAR);
+    FaceFab ef[3];
+    for (int d = 0; d < 3; ++d) ef[d].define(c->geo, d, 1);
+    solve_potential(*c, time, Sb, Sb, ef, st);
+    return VD_OK;
+}
+
+int vdo_explicit_rhs(void* ctx, double time, double* out)
+{
+    auto* c = static_cast<OCtx*>(ctx);
+    Fab Sb, rxn, expl, tmp;
+    Sb.define(c->geo, NVAR, c->ngrow);
+    rxn.define(c->geo, NUM_SPECIES + 1, 0);
+    expl.define(c->geo, NUM_SPECIES + 1, 0);
+    fill_patch(c->geo, c->phi_new, Sb, NVAR);
+    update_rxnsrc(*c, Sb, rxn, time);
+    for (int sp = 0; sp < NUM_SPECIES; ++sp)
+    {
+        if (is_bg(*c, sp)) continue;
+        update_explsrc(*c, sp, bc_lo_for(*c, sp), bc_hi_for(*c, sp), Sb, rxn, expl, time);
+    }
+    if (c->cfg.elecenergy_solve)
+        update_explsrc(*c, EEN_ID, c->cfg.eenrg_bc_lo, c->cfg.eenrg_bc_hi, Sb, rxn, expl, time);
+    std::memcpy(out, expl.d.data(), sizeof(double) * expl.d.size());
+    return VD_OK;
+}
+
+int vdo_implicit_diffusion(void* ctx, int spec, double time, const double* expl_in,
+                           vd_solve_stats* st)
+{
+    auto* c = static_cast<OCtx*>(ctx);
+    Fab Sb, expl;
+    Sb.define(c->geo, NVAR, c->ngrow);
+    expl.define(c->geo, NUM_SPECIES + 1, 0);
+    fill_patch(c->geo, c->phi_new, Sb, NVAR);
+    std::memcpy(expl.d.data(), expl_in, sizeof(double) * expl.d.size());
+    implicit_solve(*c, time, c->cfg.dt, spec, Sb, Sb, expl, bc_lo_for(*c, spec),
+                   bc_hi_for(*c, spec), nullptr, st);
+    return VD_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,165 @@
+"""Parity of the CUDA library (through the C ABI) with the CPU oracle on the
+same seeded inputs, plus the reference's known answers run on the GPU.
+
+Tolerances: the explicit sources are pointwise FP64 arithmetic and agree to
+1e-12 relative; the solves are converged to 1e-13 of the right-hand-side
+norm on both sides so the fields agree to 1e-11..1e-12 (the reference's own
+MLMG tolerance, 1e-10, would leave both sides 1e-10 apart by construction).
+Metric: the reference comparator's RMS(f1-f2)/mean|f1|
+(py_utils/compare_fields_from_twoplotfiles.py:40-46)."""
+import numpy as np
+import pytest
+
+import vidyut_b200 as vb
+from oracle.oracle import Oracle
+from tests.cases import (ADVECT_PROB, advect_config, advect_error, mms1_config,
+                         mms1_errors)
+from vidyut_b200 import workloads as W
+from vidyut_b200.compare import field_error
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = dict(linsolve_reltol=1e-13, linsolve_abstol=0.0)
+
+
+def pair(cfg, state=None, prob=None):
+    g = vb.Vidyut(cfg)
+    o = Oracle(cfg)
+    if state is not None:
+        g.set_state(0, state)
+        o.set_state(0, state)
+    if prob is not None:
+        g.init_domain(prob)
+        o.init_domain(prob)
+    return g, o
+
+
+def rel(a, b):
+    return field_error(b, a)[1]
+
+
+def townsend(dim, n, **kw):
+    cfg = W.townsend_config(dim, n)
+    for k, v in {**TIGHT, **kw}.items():
+        cfg[k] = v
+    return cfg
+
+
+@pytest.mark.parametrize("dim,n", [(2, 64), (3, 32)])
+def test_poisson_parity(require_gpu, dim, n):
+    cfg = townsend(dim, n)
+    g, o = pair(cfg, W.initial_state(cfg, 1))
+    sg = g.solve_potential(0.0)
+    so = o.solve_potential(0.0)
+    assert sg.converged and so.converged
+    info = g.info
+    Sg, So = g.get_state(), o.get_state()
+    for c in [info["pot_id"], info["efx_id"], info["efx_id"] + 1, info["ref_id"]] + \
+            ([info["efx_id"] + 2] if dim == 3 else []):
+        assert rel(Sg[c], So[c]) < 1e-11, (c, rel(Sg[c], So[c]))
+
+
+@pytest.mark.parametrize("hyp,weno", [(1, 3), (2, 3), (5, 1), (5, 2), (5, 3)])
+@pytest.mark.parametrize("dim,n", [(2, 48), (3, 24)])
+def test_explicit_rhs_parity(require_gpu, dim, n, hyp, weno):
+    cfg = townsend(dim, n, hyp_order=hyp, weno_scheme=weno)
+    state = W.initial_state(cfg, 2)
+    g, o = pair(cfg, state)
+    # a potential/field to drift in, identical on both sides
+    o.solve_potential(0.0)
+    S = o.get_state()
+    g.set_state(0, S)
+    eg, eo = g.explicit_rhs(0.0), o.explicit_rhs(0.0)
+    for c in (0, 1):
+        assert rel(eg[c], eo[c]) < 1e-12, (c, rel(eg[c], eo[c]))
+
+
+@pytest.mark.parametrize("spec", [0, 1])
+def test_implicit_diffusion_parity(require_gpu, spec):
+    cfg = townsend(3, 32)
+    g, o = pair(cfg, W.initial_state(cfg, 3))
+    o.solve_potential(0.0)
+    S = o.get_state()
+    g.set_state(0, S)
+    ex = o.explicit_rhs(0.0)
+    sg = g.implicit_solve_scalar(spec, ex, 0.0)
+    so = o.implicit_solve_scalar(spec, ex, 0.0)
+    assert sg.converged and so.converged
+    assert rel(g.get_state(spec, 1), o.get_state(spec, 1)) < 1e-12
+
+
+@pytest.mark.parametrize("dim,n,steps", [(2, 64, 4), (3, 32, 3)])
+def test_step_parity_and_invariants(require_gpu, dim, n, steps):
+    cfg = townsend(dim, n)
+    state = W.initial_state(cfg, 4)
+    g, o = pair(cfg, state)
+    info = g.info
+    for s in range(steps):
+        stg = g.step(1)
+        o.step(1)
+        Sg, So = g.get_state(), o.get_state()
+        for c in (0, 1, info["pot_id"], info["efx_id"] + dim - 1, info["etemp_id"],
+                  info["een_id"]):
+            r = rel(Sg[c], So[c])
+            assert r < 1e-11, (s, c, r)
+        # species positivity (bound_specden floors)
+        assert Sg[0].min() >= cfg["min_electron_density"]
+        assert Sg[1].min() >= cfg["min_species_density"]
+        assert stg.not_converged == 0
+    assert g.check_state() == 0
+
+
+def test_charge_conservation_reactions_only(require_gpu):
+    # ionization makes electron-ion pairs: without transport the net charge
+    # sum(n_ion - n_e) is conserved exactly up to rounding
+    cfg = townsend(3, 24, do_transport=0)
+    state = W.initial_state(cfg, 5)
+    g = vb.Vidyut(cfg)
+    g.set_state(0, state)
+    q0 = (state[1] - state[0]).sum()
+    n0 = state[0].sum()
+    g.step(3)
+    S = g.get_state(0, 2)
+    assert abs((S[1] - S[0]).sum() - q0) <= 1e-12 * n0
+
+
+def test_two_correctors_parity(require_gpu):
+    cfg = townsend(2, 48, num_timestep_correctors=2)
+    g, o = pair(cfg, W.initial_state(cfg, 6))
+    g.step(2)
+    o.step(2)
+    Sg, So = g.get_state(), o.get_state()
+    for c in (0, 1, g.info["pot_id"]):
+        assert rel(Sg[c], So[c]) < 1e-11
+
+
+def test_mms1_known_answer_on_gpu(require_gpu):
+    cfg = mms1_config(32, 5)
+    g, o = pair(cfg, prob="prob.axial_dir = 0")
+    g.step(100)
+    o.step(100)
+    en, ep = mms1_errors(g.get_state(), 32)
+    assert en < 1e-3 and ep < 1e-3
+    Sg, So = g.get_state(), o.get_state()
+    assert rel(Sg[1], So[1]) < 1e-9
+    assert rel(Sg[g.info["pot_id"]], So[g.info["pot_id"]]) < 1e-9
+
+
+@pytest.mark.parametrize("weno", [2, 3])
+def test_advect_known_answer_on_gpu(require_gpu, weno):
+    T, dt, n = 0.25, 2.5e-4, 40
+    cfg = advect_config(n, dt, weno)
+    g, o = pair(cfg, prob=ADVECT_PROB)
+    g.step(int(round(T / dt)))
+    o.step(int(round(T / dt)))
+    assert advect_error(g.get_state(), n, T) < 1e-4
+    assert rel(g.get_state(1, 1), o.get_state(1, 1)) < 1e-12
+
+
+def test_init_domain_matches_oracle(require_gpu):
+    cfg = townsend(3, 16)
+    prob = ("prob.nblobs = 2\nprob.cx = 0.005 0.012\nprob.cy = 0.01 0.01\n"
+            "prob.cz = 0.01 0.008\nprob.ampl = 1e18 3e17\nprob.sigma = 1e-3 5e-4\n")
+    g, o = pair(cfg, prob=prob)
+    assert np.array_equal(g.get_state(0, 5), o.get_state(0, 5)) or \
+        rel(g.get_state(0, 1), o.get_state(0, 1)) < 1e-14

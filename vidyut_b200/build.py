@@ -1,0 +1,78 @@
+"""Build the CUDA library, one shared object per case directory.
+
+Each case directory under ``vidyut_b200/cases/`` (the reference's per-case
+Chemistry.H / UserFunctions.H / UserSources.H / Prob.H / ProbParm.H layout)
+is compiled into ``vidyut_b200/lib/libvd_<case>.so`` for sm_100a, the way the
+reference builds one executable per case (test/Make.vidyut).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+CASES = os.path.join(PKG, "cases")
+LIBDIR = os.path.join(PKG, "lib")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC", "-shared", "-Xcudafe", "--diag_suppress=177",
+]
+
+
+def cases() -> list[str]:
+    return sorted(d for d in os.listdir(CASES)
+                  if os.path.isfile(os.path.join(CASES, d, "Chemistry.H")))
+
+
+def lib_path(case: str) -> str:
+    return os.path.join(LIBDIR, f"libvd_{case}.so")
+
+
+def sources() -> list[str]:
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))]
+
+
+def _stale(case: str) -> bool:
+    out = lib_path(case)
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    deps = sources() + [os.path.join(CASES, case, f) for f in os.listdir(os.path.join(CASES, case))]
+    deps.append(os.path.join(ROOT, "include", "vidyut_b200.h"))
+    return any(os.path.getmtime(p) > t for p in deps)
+
+
+def build_case(case: str, force: bool = False, extra: list[str] | None = None) -> str:
+    os.makedirs(LIBDIR, exist_ok=True)
+    out = lib_path(case)
+    if not force and not _stale(case):
+        return out
+    cmd = [NVCC, *NVCC_FLAGS, *(extra or []),
+           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-I", os.path.join(CASES, case),
+           f'-DVD_CASE_NAME="{case}"',
+           os.path.join(CSRC, "vd_lib.cu"), "-o", out + ".tmp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for case {case}:\n{r.stderr[-6000:]}")
+    os.replace(out + ".tmp", out)
+    return out
+
+
+def build_all(force: bool = False) -> list[str]:
+    cs = cases()
+    with ThreadPoolExecutor(max_workers=min(4, len(cs))) as ex:
+        return list(ex.map(lambda c: build_case(c, force), cs))
+
+
+if __name__ == "__main__":
+    force = "--force" in sys.argv
+    only = [a for a in sys.argv[1:] if not a.startswith("-")]
+    for c in (only or cases()):
+        print(build_case(c, force))

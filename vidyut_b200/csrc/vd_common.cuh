@@ -1,0 +1,108 @@
+// Shared device utilities of the B200 library: error checks, launch
+// accounting, block reductions, the grid descriptor.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <string>
+
+#define VD_CUDA_OK(call)                                                        \
+    do                                                                          \
+    {                                                                           \
+        cudaError_t e_ = (call);                                                \
+        if (e_ != cudaSuccess)                                                  \
+            throw vd::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace vd {
+
+struct CudaError
+{
+    std::string msg;
+    explicit CudaError(std::string m) : msg(std::move(m)) {}
+};
+
+// Grid of one multigrid level (or of the state): cell counts, active
+// dimension count, periodicity.  Index (i,j,k) -> i + nx*(j + ny*k).
+struct GridDev
+{
+    int n[3];
+    int dim;
+    int per[3];
+    __host__ __device__ long long ncell() const
+    {
+        return (long long)n[0] * n[1] * n[2];
+    }
+    __host__ __device__ long long idx(int i, int j, int k) const
+    {
+        return i + (long long)n[0] * (j + (long long)n[1] * k);
+    }
+};
+
+// Global launch counter (kernels launched by this library).
+extern long long g_launches;
+
+inline dim3 grid1d(long long n, int bs)
+{
+    long long b = (n + bs - 1) / bs;
+    if (b < 1) b = 1;
+    return dim3((unsigned)b);
+}
+
+// Max of non-negative values through their bit patterns (IEEE ordering of
+// non-negative doubles equals unsigned ordering).
+__device__ inline void atomic_max_nonneg(unsigned long long* addr, double v)
+{
+    atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename T>
+__device__ inline T warp_sum(T v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <typename T>
+__device__ inline T warp_max(T v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = v > w ? v : w;
+    }
+    return v;
+}
+
+// Block-wide sum; `sh` must hold blockDim.x/32 entries.  All threads get it.
+template <typename T>
+__device__ inline T block_sum(T v, T* sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    T r = 0;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int w = 0; w < nw; ++w) r += sh[w];
+    __syncthreads();
+    return r;
+}
+
+template <typename T>
+__device__ inline T block_max(T v, T* sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    v = warp_max(v);
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    T r = 0;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int w = 0; w < nw; ++w) r = r > sh[w] ? r : sh[w];
+    __syncthreads();
+    return r;
+}
+
+} // namespace vd

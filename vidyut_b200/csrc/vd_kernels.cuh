@@ -1,0 +1,705 @@
+// Per-step kernels of the species-and-field update (sm_100a, FP64):
+// Poisson right-hand side, boundary callbacks, electric field, the fused
+// reaction + drift-flux + divergence kernel, diffusion-solve set-up, Joule
+// heating, and the state write-back.  Each cites the reference function
+// whose arithmetic it reproduces.
+#pragma once
+
+#include "vd_mg.cuh"
+#include "vd_flux.cuh"
+
+namespace vd {
+
+#define VD_NT (NUM_SPECIES + 1)
+
+__host__ __device__ inline Array4 state_view(double* S, const GridDev& g)
+{
+    Array4 a;
+    a.p = S;
+    for (int d = 0; d < 3; ++d)
+    {
+        a.lo[d] = 0;
+        a.hi[d] = g.n[d] - 1;
+        a.periodic[d] = g.per[d];
+    }
+    a.jstride = g.n[0];
+    a.kstride = (long long)g.n[0] * g.n[1];
+    a.nstride = g.ncell();
+    a.clamp = 1;
+    return a;
+}
+
+// A view over one boundary side's plane of values, addressed by the ghost
+// cell index the reference's hooks write (face-1 low side, face high side).
+__host__ __device__ inline Array4 side_view(double* v, const GridDev& g, int s)
+{
+    const int d = s % 3;
+    Array4 a;
+    a.p = v;
+    for (int q = 0; q < 3; ++q)
+    {
+        a.lo[q] = 0;
+        a.hi[q] = g.n[q] - 1;
+    }
+    a.lo[d] = a.hi[d] = (s / 3) ? g.n[d] : -1;
+    a.jstride = a.hi[0] - a.lo[0] + 1;
+    a.kstride = a.jstride * (a.hi[1] - a.lo[1] + 1);
+    a.nstride = a.kstride * (a.hi[2] - a.lo[2] + 1);
+    return a;
+}
+
+__host__ __device__ inline Array4 cell_view(double* v, int i, int j, int k)
+{
+    Array4 a;
+    a.p = v;
+    a.lo[0] = a.hi[0] = i;
+    a.lo[1] = a.hi[1] = j;
+    a.lo[2] = a.hi[2] = k;
+    a.jstride = a.kstride = 1;
+    a.nstride = 1;
+    return a;
+}
+
+__device__ __forceinline__ int clampi(int i, int n, int per)
+{
+    if (i < 0) return per ? ((i % n) + n) % n : 0;
+    if (i >= n) return per ? i % n : n - 1;
+    return i;
+}
+
+__device__ __forceinline__ void cell_of(const GridDev& g, long long t, int& i, int& j, int& k)
+{
+    i = (int)(t % g.n[0]);
+    const long long r = t / g.n[0];
+    j = (int)(r % g.n[1]);
+    k = (int)(r / g.n[1]);
+}
+
+struct Geo
+{
+    GridDev g;
+    double dx[3];
+    double plo[3];
+    double phi[3];
+};
+
+__device__ __forceinline__ GpuArray<Real, 3> ga3(const double* v)
+{
+    GpuArray<Real, 3> a;
+    a[0] = v[0];
+    a[1] = v[1];
+    a[2] = v[2];
+    return a;
+}
+
+// ---------------- Poisson right-hand side (Source/PotentialSolve.cpp:252-277, :484)
+__global__ void k_poisson_rhs(Geo G, const double* __restrict__ Sold, double* Sv,
+                              double* __restrict__ rhs, double* __restrict__ sol,
+                              int do_spacechrg, int warm, double ps, double time,
+                              const ProbParm* pp)
+{
+    const long long N = G.g.ncell();
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        double r = 0.0;
+        if (do_spacechrg)
+        {
+#pragma unroll
+            for (int sp = 0; sp < NUM_SPECIES; sp++)
+            {
+                const int q = plasmachem::get_charge(sp);
+                if (abs(q) > 0) r += q * Sold[sp * N + t];
+            }
+            r *= (-ECHARGE / EPS0);
+#ifndef VD_NO_USER_POTENTIAL_SOURCES
+            int i, j, k;
+            cell_of(G.g, t, i, j, k);
+            Array4 sv = state_view(const_cast<double*>(Sold), G.g);
+            Array4 rv = cell_view(&r, i, j, k);
+            user_sources::add_user_potential_sources(i, j, k, sv, rv, ga3(G.plo), ga3(G.phi),
+                                                     ga3(G.dx), time, *pp);
+#endif
+        }
+        rhs[t] = r * (1.0 / ps);
+        sol[t] = warm ? Sv[POT_ID * N + t] / ps : 0.0;
+    }
+}
+
+// ---------------- boundary callbacks (Source/PotentialSolve.cpp:350-434,
+// Source/ScalarSolve.cpp:693-803): one thread per face of side s.
+struct SideArrays
+{
+    double* val;
+    double* ra;
+    double* rb;
+    double* rf;
+    double* g;
+    double* c0;
+};
+
+__global__ void k_bc_hook(Geo G, int s, int kind, int comp, double* S, SideArrays A,
+                          double time, double app_voltage, int user_defined, double Tg,
+                          double Pg, const ProbParm* pp)
+{
+    const int d = s % 3;
+    const int ta = (d == 0) ? 1 : 0, tb = (d == 2) ? 1 : 2;
+    const int np = G.g.n[ta] * G.g.n[tb];
+    const int sgn = (s / 3) ? 1 : -1;
+    const long long N = G.g.ncell();
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x)
+    {
+        int c[3], f[3];
+        c[d] = (s / 3) ? G.g.n[d] - 1 : 0;
+        c[ta] = q % G.g.n[ta];
+        c[tb] = q / G.g.n[ta];
+        f[0] = c[0];
+        f[1] = c[1];
+        f[2] = c[2];
+        f[d] = (s / 3) ? G.g.n[d] : 0;
+        A.val[q] = S[comp * N + G.g.idx(c[0], c[1], c[2])];
+        A.ra[q] = 0.0;
+        A.rb[q] = 1.0;
+        A.rf[q] = 0.0;
+        Array4 sv = state_view(S, G.g);
+        Array4 bv = side_view(A.val, G.g, s), av = side_view(A.ra, G.g, s),
+               bbv = side_view(A.rb, G.g, s), fv = side_view(A.rf, G.g, s);
+        if (kind == 0)
+        {
+#ifdef VD_HAS_USER_TRANSPORT
+            if (user_defined)
+                user_transport::potential_bc(f[0], f[1], f[2], d, sgn, sv, bv, av, bbv, fv,
+                                             ga3(G.plo), ga3(G.phi), ga3(G.dx), time, *pp, Tg,
+                                             Pg, app_voltage);
+            else
+#endif
+                plasmachem_transport::potential_bc(f[0], f[1], f[2], d, sgn, sv, bv, av, bbv,
+                                                   fv, ga3(G.plo), ga3(G.phi), ga3(G.dx), time,
+                                                   *pp, Tg, Pg, app_voltage);
+        } else
+        {
+#ifdef VD_HAS_USER_TRANSPORT
+            if (user_defined)
+                user_transport::species_bc(f[0], f[1], f[2], d, sgn, comp, 0, sv, bv, av, bbv,
+                                           fv, ga3(G.plo), ga3(G.phi), ga3(G.dx), time, *pp,
+                                           Tg, Pg);
+            else
+#endif
+                plasmachem_transport::species_bc(f[0], f[1], f[2], d, sgn, comp, 0, sv, bv, av,
+                                                 bbv, fv, ga3(G.plo), ga3(G.phi), ga3(G.dx),
+                                                 time, *pp, Tg, Pg);
+        }
+    }
+}
+
+// Scale the hook values into the solver's units and turn them into the
+// ghost affine form (g = inhomogeneous part, c0 = Robin interior factor).
+__global__ void k_bc_finalize(int np, int type, int nx_d, int maxorder, double dx,
+                              double scale, SideArrays A)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x)
+    {
+        A.val[q] *= scale;
+        A.rf[q] *= scale;
+        if (type == MG_DIR)
+        {
+            const int NX = min(nx_d + 1, maxorder);
+            A.g[q] = (NX <= 2) ? 2.0 * A.val[q] : (8.0 / 3.0) * A.val[q];
+        } else if (type == MG_ROBIN)
+        {
+            const double a = A.ra[q], b = A.rb[q], dxi = 1.0 / dx;
+            const double den = 0.5 * a + b * dxi;
+            A.c0[q] = (b * dxi - 0.5 * a) / den;
+            A.g[q] = A.rf[q] / den;
+        } else
+        {
+            A.g[q] = 0.0;
+        }
+    }
+}
+
+// Inhomogeneous Neumann: the face gradient enters the right-hand side.
+__global__ void k_inneu_adjust(GridDev g, int s, const double* bface, double bconst,
+                               double beta, double dx, const double* val,
+                               double* __restrict__ rhs)
+{
+    const int d = s % 3;
+    const int ta = (d == 0) ? 1 : 0, tb = (d == 2) ? 1 : 2;
+    const int np = g.n[ta] * g.n[tb];
+    const bool hi = (s / 3) != 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x)
+    {
+        int c[3];
+        c[d] = hi ? g.n[d] - 1 : 0;
+        c[ta] = q % g.n[ta];
+        c[tb] = q / g.n[ta];
+        int f[3] = {c[0], c[1], c[2]};
+        if (hi) f[d] += 1;
+        const double b = bface ? bface[face_index(g, d, f[0], f[1], f[2])] : bconst;
+        const double fac = beta / dx;
+        rhs[g.idx(c[0], c[1], c[2])] += (hi ? 1.0 : -1.0) * fac * b * val[q];
+    }
+}
+
+// Face gradient of a solved field with its boundary closure (MLMG
+// getGradSolution); inhomogeneous-Neumann faces return their gradient.
+struct GradCtx
+{
+    MGOp<double> op; // fine operator of the solve (boundary data)
+    double dxi[3];
+    const double* inneu_val[6];
+};
+
+__device__ __forceinline__ double grad_at_face(const GradCtx& C, const double* __restrict__ x,
+                                               int d, int i, int j, int k)
+{
+    const GridDev& g = C.op.g;
+    int c[3] = {i, j, k};
+    const int fi = c[d];
+    if (fi > 0 && fi < g.n[d])
+    {
+        int m[3] = {i, j, k};
+        m[d] -= 1;
+        return (x[g.idx(i, j, k)] - x[g.idx(m[0], m[1], m[2])]) * C.dxi[d];
+    }
+    if (g.per[d])
+    {
+        int m[3] = {i, j, k}, p[3] = {i, j, k};
+        m[d] = g.n[d] - 1;
+        p[d] = 0;
+        return (x[g.idx(p[0], p[1], p[2])] - x[g.idx(m[0], m[1], m[2])]) * C.dxi[d];
+    }
+    const bool lo = (fi == 0);
+    int in[3] = {i, j, k};
+    if (!lo) in[d] -= 1;
+    const int s = d + (lo ? 0 : 3);
+    if (C.op.bct[s] == MG_INNEU) return C.inneu_val[s][plane_index(g, d, in[0], in[1], in[2])];
+    const double x0 = x[g.idx(in[0], in[1], in[2])];
+    double cf;
+    const double gh = mg_nbr(C.op, x, in[0], in[1], in[2], d, lo ? -1 : 1, true, x0, cf);
+    return lo ? (x0 - gh) * C.dxi[d] : (gh - x0) * C.dxi[d];
+}
+
+// ---------------- E field, reduced field, potential (Source/PotentialSolve.cpp:500-541)
+__global__ void k_efield(GradCtx C, const double* __restrict__ sol, double* __restrict__ S,
+                         double ps)
+{
+    const GridDev& g = C.op.g;
+    const long long N = g.ncell();
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        cell_of(g, t, i, j, k);
+        double E[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < g.dim; ++d)
+        {
+            int p[3] = {i, j, k};
+            p[d] += 1;
+            const double flo = grad_at_face(C, sol, d, i, j, k) * (-1.0 * ps);
+            const double fhi = grad_at_face(C, sol, d, p[0], p[1], p[2]) * (-1.0 * ps);
+            E[d] = 0.5 * (flo + fhi);
+            S[(EFX_ID + d) * N + t] = E[d];
+        }
+        double Esum = 0.0, nd = 0.0;
+#pragma unroll
+        for (int sp = 0; sp < NUM_SPECIES; sp++) nd += S[sp * N + t];
+        nd = nd - S[E_ID * N + t];
+        for (int d = 0; d < g.dim; ++d) Esum += E[d] * E[d];
+        S[REF_ID * N + t] = (sqrt(Esum) / nd) / 1.0e-21;
+        S[POT_ID * N + t] = sol[t] * ps;
+    }
+}
+
+// ---------------- fused reactions + drift flux + divergence
+// (update_rxnsrc_at_all_levels, Source/ScalarSolve.cpp:181-209;
+//  compute_scalar_transport_flux + compute_flux, Source/ScalarSolve.cpp:285-324,
+//  Source/compute_explicit_flux.H:218-415; compute_dsdt, Source/ScalarSolve.cpp:50-78).
+// Every transported component's explicit source in one pass over the cells;
+// each thread evaluates its cell's low and high faces in every direction.
+struct ExplParams
+{
+    Geo G;
+    const double* S;
+    double* expl;
+    double* rxn_een;
+    double Tg, Pg, time, dt, dxmin;
+    int hyp_order, weno_scheme, user_vel, do_transport, do_reactions, do_bg_rxn;
+    int ntr;
+    int comp[VD_NT];
+    int bclo[VD_NT][3];
+    int bchi[VD_NT][3];
+    int bg[NUM_SPECIES];
+    const ProbParm* pp;
+};
+
+__device__ __forceinline__ bool wall_zero(int code) { return code == IHNEUBC || code == AXISBC; }
+
+__global__ void __launch_bounds__(256) k_explicit(ExplParams P)
+{
+    const GridDev& g = P.G.g;
+    const long long N = g.ncell();
+    const double* __restrict__ S = P.S;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        int c3[3];
+        cell_of(g, t, c3[0], c3[1], c3[2]);
+        double rx[VD_NT];
+#pragma unroll
+        for (int q = 0; q < VD_NT; ++q) rx[q] = 0.0;
+        if (P.do_reactions)
+        {
+            double C[NUM_SPECIES], W[NUM_SPECIES];
+#pragma unroll
+            for (int sp = 0; sp < NUM_SPECIES; sp++) C[sp] = S[sp * N + t] / N_A;
+            double ee = 0.0;
+            CKWC(P.Tg, C, W, S[ETEMP_ID * N + t], S[REF_ID * N + t], &ee);
+#pragma unroll
+            for (int sp = 0; sp < NUM_SPECIES; sp++) rx[sp] = W[sp] * N_A;
+            rx[NUM_SPECIES] = ee;
+#ifndef VD_NO_USER_REACT_SOURCES
+            Array4 sv = state_view(const_cast<double*>(S), g);
+            Array4 rv = cell_view(rx, c3[0], c3[1], c3[2]);
+            user_sources::add_user_react_sources(c3[0], c3[1], c3[2], sv, rv, ga3(P.G.plo),
+                                                 ga3(P.G.phi), ga3(P.G.dx), P.time, *P.pp,
+                                                 P.Tg, P.Pg);
+#endif
+        }
+        if (P.rxn_een) P.rxn_een[t] = rx[NUM_SPECIES];
+        for (int sp = 0; sp < NUM_SPECIES; sp++)
+            if (P.bg[sp]) P.expl[sp * N + t] = P.do_bg_rxn ? rx[sp] : 0.0;
+
+        double acc[VD_NT];
+        for (int q = 0; q < P.ntr; ++q) acc[q] = 0.0;
+        for (int d = 0; d < g.dim && P.do_transport; ++d)
+        {
+            // per stencil position: cell index, Te, heavy sum, |E|, E_d
+            long long qi[7];
+            double te[7], nd[7], em[7], ed[7];
+            for (int m = 0; m < 7; ++m)
+            {
+                int c[3] = {c3[0], c3[1], c3[2]};
+                c[d] = clampi(c[d] + m - 3, g.n[d], g.per[d]);
+                const long long q = g.idx(c[0], c[1], c[2]);
+                qi[m] = q;
+                const double ex = S[EFX_ID * N + q], ey = S[EFY_ID * N + q],
+                             ez = S[EFZ_ID * N + q];
+                em[m] = sqrt(ex * ex + ey * ey + ez * ez);
+                ed[m] = S[(EFX_ID + d) * N + q];
+                te[m] = S[ETEMP_ID * N + q];
+                double s = 0.0;
+#pragma unroll
+                for (int sp = 0; sp < NUM_SPECIES; sp++) s += S[sp * N + q];
+                nd[m] = s;
+            }
+            for (int q = 0; q < P.ntr; ++q)
+            {
+                const int comp = P.comp[q];
+                double u[7], v[7];
+                for (int m = 0; m < 7; ++m)
+                {
+                    u[m] = S[comp * N + qi[m]];
+#ifdef VD_HAS_USER_TRANSPORT
+                    if (P.user_vel)
+                    {
+                        int c[3] = {c3[0], c3[1], c3[2]};
+                        c[d] += m - 3;
+                        Array4 sv = state_view(const_cast<double*>(S), g);
+                        v[m] = user_transport::compute_vel(IntVect{c[0], c[1], c[2]}, d, comp,
+                                                           sv, ga3(P.G.dx), P.time, *P.pp,
+                                                           P.Tg, P.Pg);
+                    } else
+#endif
+                        v[m] = specMob(comp, te[m], nd[m], em[m], P.Tg) * ed[m];
+                }
+                double flo = face_flux6(u, v, P.hyp_order, P.weno_scheme, P.dxmin, P.dt);
+                double fhi = face_flux6(u + 1, v + 1, P.hyp_order, P.weno_scheme, P.dxmin, P.dt);
+                if (c3[d] == 0 && wall_zero(P.bclo[q][d])) flo = 0.0;
+                if (c3[d] == g.n[d] - 1 && wall_zero(P.bchi[q][d])) fhi = 0.0;
+                if (d == 0)
+                    acc[q] = (flo - fhi) / P.G.dx[0] + rx[comp];
+                else
+                    acc[q] += (flo - fhi) / P.G.dx[d];
+            }
+        }
+        for (int q = 0; q < P.ntr; ++q)
+        {
+            const int comp = P.comp[q];
+            P.expl[comp * N + t] = P.do_transport ? acc[q] : rx[comp];
+        }
+    }
+}
+
+// ---------------- diffusion-solve set-up (Source/ScalarSolve.cpp:587-690, :819-846)
+__device__ __forceinline__ double cell_diff(const double* __restrict__ S, const GridDev& g,
+                                            long long N, int spec, int i, int j, int k,
+                                            double Tg)
+{
+    const long long q = g.idx(clampi(i, g.n[0], g.per[0]), clampi(j, g.n[1], g.per[1]),
+                              clampi(k, g.n[2], g.per[2]));
+    double Es = 0.0, nd = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+        const double e = S[(EFX_ID + d) * N + q];
+        Es += e * e;
+    }
+    const double emag = sqrt(Es);
+#pragma unroll
+    for (int sp = 0; sp < NUM_SPECIES; sp++) nd += S[sp * N + q];
+    return specDiff(spec, S[ETEMP_ID * N + q], nd, emag, Tg);
+}
+
+// Harmonic face average of the cell diffusivity (0 where both cells are 0).
+__global__ void k_species_faces(GridDev g, int d, const double* __restrict__ S, int spec,
+                                double Tg, double* __restrict__ bf)
+{
+    const long long tot = face_count(g, d);
+    const long long N = g.ncell();
+    const int nx = g.n[0] + (d == 0), ny = g.n[1] + (d == 1);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        const int i = (int)(t % nx);
+        const long long r = t / nx;
+        const int j = (int)(r % ny);
+        const int k = (int)(r / ny);
+        int m[3] = {i, j, k};
+        m[d] -= 1;
+        const double d0 = cell_diff(S, g, N, spec, m[0], m[1], m[2], Tg);
+        const double d1 = cell_diff(S, g, N, spec, i, j, k, Tg);
+        const double den = d0 + d1;
+        bf[t] = (den != 0.0) ? 2.0 * d0 * d1 / den : 0.0;
+    }
+}
+
+__global__ void k_species_rhs(GridDev g, const double* __restrict__ S,
+                              const double* __restrict__ Sold, const double* __restrict__ expl,
+                              int spec, double dt, double ts, double scale,
+                              double* __restrict__ rhs, double* __restrict__ sol)
+{
+    const long long N = g.ncell();
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        const double r = (1.0 / dt) * Sold[spec * N + t] + 1.0 * expl[spec * N + t];
+        rhs[t] = r * (ts / scale);
+        sol[t] = S[spec * N + t] * (1.0 / scale);
+    }
+}
+
+// ---------------- Joule heating (Source/ElecEnergySource.cpp:127-293)
+struct JouleParams
+{
+    GradCtx pot;           // Poisson boundary data, for the face field
+    const double* phi_sol; // scaled Poisson solution
+    double ps;
+    const double* ue;      // electron solution (scaled, before the floor)
+    double escale;
+    const double* S;
+    double* expl;
+    double* ejh;
+    double dx[3];
+    double Tg;
+    int floor_jh;
+    int eidx;
+};
+
+__device__ __forceinline__ double onesided_grad(const double* S, const GridDev& g, long long N,
+                                                int comp, const int* face, int sgn, int d,
+                                                double dx)
+{
+    int cell[3] = {face[0], face[1], face[2]};
+    cell[d] += (sgn == 1) ? -1 : 0;
+    int n1[3] = {cell[0], cell[1], cell[2]}, n2[3] = {cell[0], cell[1], cell[2]};
+    n1[d] = cell[d] - sgn;
+    n2[d] = n1[d] - sgn;
+    auto at = [&](const int* c) {
+        return S[comp * N + g.idx(clampi(c[0], g.n[0], g.per[0]), clampi(c[1], g.n[1], g.per[1]),
+                                  clampi(c[2], g.n[2], g.per[2]))];
+    };
+    double g1, g2;
+    if (sgn == -1)
+    {
+        g1 = (at(n1) - at(cell)) / dx;
+        g2 = (at(n2) - at(n1)) / dx;
+    } else
+    {
+        g1 = (at(cell) - at(n1)) / dx;
+        g2 = (at(n1) - at(n2)) / dx;
+    }
+    return 2.0 * g1 - g2;
+}
+
+__global__ void k_joule(JouleParams P)
+{
+    const GridDev& g = P.pot.op.g;
+    const long long N = g.ncell();
+    const double* __restrict__ S = P.S;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        int c3[3];
+        cell_of(g, t, c3[0], c3[1], c3[2]);
+        const double charge = plasmachem::get_charge(P.eidx) * ECHARGE;
+        double jh = 0.0;
+        for (int d = 0; d < g.dim; ++d)
+            for (int f = 0; f < 2; ++f)
+            {
+                int face[3] = {c3[0], c3[1], c3[2]};
+                face[d] += f;
+                int lc[3] = {face[0], face[1], face[2]};
+                lc[d] -= 1;
+                const long long ql = g.idx(clampi(lc[0], g.n[0], g.per[0]),
+                                           clampi(lc[1], g.n[1], g.per[1]),
+                                           clampi(lc[2], g.n[2], g.per[2]));
+                const long long qr = g.idx(clampi(face[0], g.n[0], g.per[0]),
+                                           clampi(face[1], g.n[1], g.per[1]),
+                                           clampi(face[2], g.n[2], g.per[2]));
+                const double te = (S[ETEMP_ID * N + ql] + S[ETEMP_ID * N + qr]) / 2.0;
+                double Esum = 0.0;
+                for (int q = 0; q < g.dim; ++q)
+                {
+                    const double e = (S[(EFX_ID + q) * N + ql] + S[(EFX_ID + q) * N + qr]) / 2.0;
+                    Esum += e * e;
+                }
+                const double emag = sqrt(Esum);
+                const double ne = (S[P.eidx * N + ql] + S[P.eidx * N + qr]) / 2.0;
+                const double ef =
+                    grad_at_face(P.pot, P.phi_sol, d, face[0], face[1], face[2]) * (-1.0 * P.ps);
+                double nd = 0.0;
+#pragma unroll
+                for (int sp = 0; sp < NUM_SPECIES; sp++) nd += (S[sp * N + ql] + S[sp * N + qr]) / 2.0;
+                const double mu = specMob(P.eidx, te, nd, emag, P.Tg);
+                const double dc = specDiff(P.eidx, te, nd, emag, P.Tg);
+                double gn;
+                if (face[d] == 0 || face[d] == g.n[d])
+                {
+                    const int sgn = (face[d] == 0) ? -1 : 1;
+                    gn = onesided_grad(S, g, N, P.eidx, face, sgn, d, P.dx[d]);
+                } else
+                {
+                    gn = (P.ue[qr] - P.ue[ql]) * (1.0 / P.dx[d]) * P.escale;
+                }
+                const double cd = charge * (mu * ne * ef - dc * gn);
+                jh += cd * ef;
+            }
+        jh *= 0.5;
+        if (P.floor_jh && jh < 0.0) jh = 0.0;
+        P.expl[NUM_SPECIES * N + t] += jh;
+        P.ejh[t] = jh;
+    }
+}
+
+// ---------------- write-back of the solves into the state
+// (Source/ScalarSolve.cpp:894-987, Source/ElecEnergySource.cpp:43-69,
+//  Source/Evolve.cpp:432-456)
+struct FinalParams
+{
+    GridDev g;
+    double* S;
+    int nsol;
+    int comp[VD_NT];
+    const double* u[VD_NT];
+    double scale[VD_NT];
+    int bound_specden;
+    double min_e, min_s, min_te;
+    int eidx;
+    int een_solved;
+    int heat_diag;
+    int lfa;
+    double Tg;
+    const double* ejh;
+    const double* rxn_een;
+    const double* expl;
+    int bg[NUM_SPECIES];
+    int do_bg_rxn;
+    double dt;
+};
+
+__global__ void k_finalize(FinalParams P)
+{
+    const long long N = P.g.ncell();
+    double* __restrict__ S = P.S;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        // values of the iteration's starting state read before any write
+        double spec_old[NUM_SPECIES];
+#pragma unroll
+        for (int sp = 0; sp < NUM_SPECIES; sp++) spec_old[sp] = S[sp * N + t];
+        const double ref_old = S[REF_ID * N + t];
+        const double cmask = S[CMASK_ID * N + t];
+        for (int q = 0; q < P.nsol; ++q)
+        {
+            const int c = P.comp[q];
+            double v = P.u[q][t] * P.scale[q];
+            if (P.bound_specden && c != EEN_ID)
+            {
+                if (c == P.eidx)
+                {
+                    if (v < P.min_e) v = P.min_e;
+                } else if (v < P.min_s)
+                    v = P.min_s;
+            }
+            S[c * N + t] = v;
+        }
+        for (int sp = 0; sp < NUM_SPECIES; sp++)
+            if (P.bg[sp] && P.do_bg_rxn)
+            {
+                double v = S[sp * N + t] + P.expl[sp * N + t] * P.dt;
+                if (v < P.min_s && P.bound_specden) v = P.min_s;
+                S[sp * N + t] = v;
+            }
+        const double ne_new = S[P.eidx * N + t];
+        if (P.een_solved)
+        {
+            const double te = twothird / K_B * S[EEN_ID * N + t] / spec_old[P.eidx];
+            S[ETEMP_ID * N + t] = te;
+            if (te < P.min_te)
+            {
+                S[ETEMP_ID * N + t] = P.min_te;
+                S[EEN_ID * N + t] = 1.5 * K_B * ne_new * P.min_te;
+            }
+        }
+        if (P.heat_diag)
+        {
+            S[EJH_ID * N + t] = P.ejh[t];
+            S[EIH_ID * N + t] = P.rxn_een[t];
+        }
+        if (P.lfa && int(cmask))
+        {
+            double te = etempLFA(P.Tg, spec_old, ref_old);
+            if (te < P.min_te) te = P.min_te;
+            S[ETEMP_ID * N + t] = te;
+            S[EEN_ID * N + t] = 1.5 * K_B * ne_new * P.min_te;
+        }
+    }
+}
+
+__global__ void k_midpoint(double* __restrict__ S, const double* __restrict__ Sold, long long n)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        S[t] = 0.5 * Sold[t] + 0.5 * S[t];
+}
+
+__global__ void k_nonfinite(const double* __restrict__ S, long long n, unsigned long long* cnt)
+{
+    unsigned long long c = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        if (!isfinite(S[t])) ++c;
+    if (c) atomicAdd(cnt, c);
+}
+
+template <typename T>
+__global__ void k_add_scaled(double* __restrict__ x, const T* __restrict__ e, double s, long long n)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        x[t] += (double)e[t] * s;
+}
+
+} // namespace vd

@@ -1,0 +1,1324 @@
+// B200-native per-timestep species-and-field update of Vidyut3d on one
+// uniform level: host driver and C ABI (include/vidyut_b200.h).
+//
+// One translation unit per case directory (-I <case>): the case's hook
+// headers are compiled into every kernel, as the reference compiles one
+// executable per case.  All device memory is allocated in vd_create; a
+// step allocates nothing.  Work is ordered on one CUDA stream per context.
+#include <vidyut_b200.h>
+
+#include "vd_vars.H"
+#include "vd_parmparse.H"
+#include "PlasmaChem.H"
+#include <UserFunctions.H>
+#include <UserSources.H>
+#include <Prob.H>
+
+#include "vd_common.cuh"
+#include "vd_kernels.cuh"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace vd {
+long long g_launches = 0;
+}
+using namespace vd;
+
+namespace {
+
+constexpr int BS = 256;
+
+dim3 gsz(long long n)
+{
+    long long b = (n + BS - 1) / BS;
+    if (b < 1) b = 1;
+    if (b > 148LL * 32) b = 148LL * 32;
+    return dim3((unsigned)b);
+}
+
+#define LAUNCH(K, G, B, STREAM, ...)                                              \
+    do                                                                            \
+    {                                                                             \
+        K<<<(G), (B), 0, (STREAM)>>>(__VA_ARGS__);                                \
+        ++vd::g_launches;                                                         \
+        VD_CUDA_OK(cudaGetLastError());                                           \
+    } while (0)
+
+// Launch-by-launch event timing of one selected kernel.
+struct Prof
+{
+    int id = VD_PROF_NONE;
+    std::vector<cudaEvent_t> a, b;
+    int n = 0;
+    double bytes = 0.0;
+    void begin(cudaStream_t st)
+    {
+        if (n >= (int)a.size())
+        {
+            cudaEvent_t x, y;
+            VD_CUDA_OK(cudaEventCreate(&x));
+            VD_CUDA_OK(cudaEventCreate(&y));
+            a.push_back(x);
+            b.push_back(y);
+        }
+        VD_CUDA_OK(cudaEventRecord(a[n], st));
+    }
+    void end(cudaStream_t st)
+    {
+        VD_CUDA_OK(cudaEventRecord(b[n], st));
+        ++n;
+    }
+};
+thread_local Prof* t_prof = nullptr;
+
+struct Alloc
+{
+    std::vector<void*> ptrs;
+    template <class T>
+    T* get(size_t n)
+    {
+        if (n == 0) n = 1;
+        void* p = nullptr;
+        if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess)
+            throw CudaError("cudaMalloc of " + std::to_string(n * sizeof(T)) + " bytes failed");
+        ptrs.push_back(p);
+        return static_cast<T*>(p);
+    }
+    void release()
+    {
+        for (void* p : ptrs) cudaFree(p);
+        ptrs.clear();
+    }
+};
+
+int mg_type(int code)
+{
+    switch (code)
+    {
+    case PERBC: return MG_PER;
+    case DIRCBC: return MG_DIR;
+    case HNEUBC: return MG_NEU;
+    case IHNEUBC: return MG_INNEU;
+    case ROBINBC: return MG_ROBIN;
+    case AXISBC: return MG_NEU;
+    default: return MG_ROBIN;
+    }
+}
+
+// ------------------------------------------------------------ hierarchy
+template <typename T>
+struct Hier
+{
+    int nlev = 0;
+    int dim = 3;
+    bool varb = false;
+    std::vector<GridDev> g;
+    std::vector<std::array<double, 3>> dx;
+    std::vector<T*> x, f;
+    std::vector<std::array<T*, 3>> bf;
+    std::vector<std::array<T*, 6>> ra, rb, c0;
+    std::array<T*, 6> g0{};
+    T* t0x = nullptr; // level-0 correction when there is a single level
+    T* t0f = nullptr;
+    T* scratch = nullptr;
+    int* status = nullptr;
+    std::vector<MGOp<T>> op;
+    int prof_tag = VD_PROF_NONE; // profiling id of this hierarchy's fine sweeps
+    int nu1 = 2, nu2 = 2, nub = 0, nuf = 8, bot_maxiter = 200;
+    double bot_rel = 1e-4;
+};
+
+template <typename T>
+void hier_build(Hier<T>& H, Alloc& A, const GridDev& fine, const double* dx, int maxcoarsen,
+                bool varb, bool own0)
+{
+    H.dim = fine.dim;
+    H.varb = varb;
+    H.g.push_back(fine);
+    H.dx.push_back({dx[0], dx[1], dx[2]});
+    while ((int)H.g.size() - 1 < maxcoarsen)
+    {
+        const GridDev& c = H.g.back();
+        bool ok = true;
+        for (int d = 0; d < H.dim; ++d)
+            if (c.n[d] % 2 != 0 || c.n[d] / 2 < 2) ok = false;
+        if (!ok) break;
+        GridDev n = c;
+        std::array<double, 3> ndx = H.dx.back();
+        for (int d = 0; d < H.dim; ++d)
+        {
+            n.n[d] = c.n[d] / 2;
+            ndx[d] = ndx[d] * 2.0;
+        }
+        H.g.push_back(n);
+        H.dx.push_back(ndx);
+    }
+    H.nlev = (int)H.g.size();
+    H.x.assign(H.nlev, nullptr);
+    H.f.assign(H.nlev, nullptr);
+    H.bf.assign(H.nlev, {nullptr, nullptr, nullptr});
+    H.ra.assign(H.nlev, {});
+    H.rb.assign(H.nlev, {});
+    H.c0.assign(H.nlev, {});
+    for (int l = 0; l < H.nlev; ++l)
+    {
+        const long long n = H.g[l].ncell();
+        if (l > 0 || own0)
+        {
+            H.x[l] = A.get<T>(n);
+            H.f[l] = A.get<T>(n);
+        }
+        if (varb)
+            for (int d = 0; d < H.dim; ++d) H.bf[l][d] = A.get<T>(face_count(H.g[l], d));
+        for (int s = 0; s < 6; ++s)
+        {
+            const int np = plane_count(H.g[l], s % 3);
+            H.ra[l][s] = A.get<T>(np);
+            H.rb[l][s] = A.get<T>(np);
+            H.c0[l][s] = A.get<T>(np);
+        }
+    }
+    for (int s = 0; s < 6; ++s) H.g0[s] = A.get<T>(plane_count(fine, s % 3));
+    if (H.nlev == 1)
+    {
+        H.t0x = A.get<T>(fine.ncell());
+        H.t0f = A.get<T>(fine.ncell());
+    }
+    H.scratch = A.get<T>(6 * H.g.back().ncell());
+    H.status = A.get<int>(1);
+}
+
+template <typename T>
+void hier_set_ops(Hier<T>& H, double aconst, double beta, double bconst, const int* bct,
+                  int maxorder)
+{
+    H.op.assign(H.nlev, MGOp<T>{});
+    for (int l = 0; l < H.nlev; ++l)
+    {
+        MGOp<T>& o = H.op[l];
+        o.g = H.g[l];
+        for (int d = 0; d < 3; ++d)
+            o.dh[d] = (d < H.dim) ? T(beta / (H.dx[l][d] * H.dx[l][d])) : T(0);
+        o.aconst = T(aconst);
+        o.a = nullptr;
+        for (int d = 0; d < 3; ++d) o.b[d] = (H.varb && d < H.dim) ? H.bf[l][d] : nullptr;
+        o.bconst = T(bconst);
+        for (int s = 0; s < 6; ++s)
+        {
+            const int d = s % 3;
+            o.bct[s] = bct[s];
+            o.c0s[s] = T(1);
+            o.c1s[s] = T(0);
+            o.c0[s] = nullptr;
+            o.gv[s] = nullptr;
+            if (bct[s] == MG_DIR)
+            {
+                const int NX = std::min(H.g[l].n[d] + 1, maxorder);
+                o.c0s[s] = (NX <= 2) ? T(-1) : T(-2);
+                o.c1s[s] = (NX <= 2) ? T(0) : T(1.0 / 3.0);
+                if (l == 0) o.gv[s] = H.g0[s];
+            } else if (bct[s] == MG_ROBIN)
+            {
+                o.c0[s] = H.c0[l][s];
+                if (l == 0) o.gv[s] = H.g0[s];
+            }
+        }
+    }
+}
+
+template <typename T>
+void hier_coarsen_coeffs(Hier<T>& H, const int* bct, cudaStream_t st)
+{
+    for (int l = 1; l < H.nlev; ++l)
+    {
+        if (H.varb)
+            for (int d = 0; d < H.dim; ++d)
+                LAUNCH(k_mg_avg_faces<T>, gsz(face_count(H.g[l], d)), BS, st, H.g[l - 1],
+                       H.g[l], d, H.bf[l - 1][d], H.bf[l][d]);
+        for (int s = 0; s < 6; ++s)
+            if (bct[s] == MG_ROBIN)
+                LAUNCH(k_mg_robin_coarsen<T>, gsz(plane_count(H.g[l], s % 3)), BS, st,
+                       H.g[l - 1], H.g[l], s, H.ra[l - 1][s], H.rb[l - 1][s], H.ra[l][s],
+                       H.rb[l][s], H.c0[l][s], T(H.dx[l][s % 3]));
+    }
+}
+
+template <typename T>
+void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t st,
+            int prof_tag = VD_PROF_NONE)
+{
+    const long long half = (long long)((op.g.n[0] + 1) / 2) * op.g.n[1] * op.g.n[2];
+    const bool prof = t_prof && prof_tag != VD_PROF_NONE && t_prof->id == prof_tag;
+    if (prof) t_prof->bytes = double(2 * sizeof(T)) * (double)op.g.ncell();
+    for (int s = 0; s < n; ++s)
+        for (int color = 0; color < 2; ++color)
+        {
+            if (prof) t_prof->begin(st);
+            LAUNCH(k_mg_smooth_color<T>, gsz(half), BS, st, op, x, f, color, inh ? 1 : 0);
+            if (prof) t_prof->end(st);
+        }
+}
+
+template <typename T>
+void bottom(Hier<T>& H, const MGOp<T>& op, T* x, const T* f, cudaStream_t st)
+{
+    LAUNCH(k_mg_bottom<T>, 1, 256, st, op, x, f, H.scratch, T(H.bot_rel), H.bot_maxiter,
+           H.nub, H.nuf, H.status);
+}
+
+// One V-cycle on level-0 unknown x0 with right-hand side f0; the level-0
+// boundary data is inhomogeneous when `inh0` (the solution itself is
+// smoothed), homogeneous otherwise (a correction is smoothed).
+template <typename T>
+void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaStream_t st)
+{
+    const int L = H.nlev;
+    if (L == 1)
+    {
+        LAUNCH(k_mg_resid_norm<T>, gsz(H.g[0].ncell()), BS, st, H.op[0], x0, f0, H.t0f, dscr,
+               inh0 ? 1 : 0);
+        bottom(H, H.op[0], H.t0x, H.t0f, st);
+        LAUNCH(k_mg_prolong_add<T>, gsz(H.g[0].ncell()), BS, st, H.g[0], H.g[0], x0, H.t0x);
+        return;
+    }
+    for (int l = 0; l < L - 1; ++l)
+    {
+        T* xl = l ? H.x[l] : x0;
+        T* fl = l ? H.f[l] : f0;
+        const bool inh = (l == 0) && inh0;
+        smooth(H.op[l], xl, fl, inh, H.nu1, st, l == 0 ? H.prof_tag : VD_PROF_NONE);
+        LAUNCH(k_mg_resid_restrict<T>, gsz(H.g[l + 1].ncell()), BS, st, H.op[l], xl, fl,
+               H.g[l + 1], H.f[l + 1], H.x[l + 1], inh ? 1 : 0);
+    }
+    bottom(H, H.op[L - 1], H.x[L - 1], H.f[L - 1], st);
+    for (int l = L - 2; l >= 0; --l)
+    {
+        T* xl = l ? H.x[l] : x0;
+        T* fl = l ? H.f[l] : f0;
+        const bool inh = (l == 0) && inh0;
+        LAUNCH(k_mg_prolong_add<T>, gsz(H.g[l].ncell()), BS, st, H.g[l], H.g[l + 1], xl,
+               H.x[l + 1]);
+        smooth(H.op[l], xl, fl, inh, H.nu2, st, l == 0 ? H.prof_tag : VD_PROF_NONE);
+    }
+}
+
+// ------------------------------------------------------------ context
+struct Ctx
+{
+    vd_config cfg{};
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    Geo G{};
+    GridDev g{};
+    long long N = 0;
+    Alloc A;
+    double* S = nullptr;
+    double* Sold = nullptr; // separate copy only with >1 corrector
+    double* expl = nullptr;
+    double* rxn_een = nullptr;
+    double* ejh = nullptr;
+    double* u[VD_NT] = {};   // solve outputs, indexed by component
+    double* phi_sol = nullptr;
+    double* phi_rhs = nullptr;
+    double* spec_rhs = nullptr;
+    double* r64 = nullptr;  // FP64 residual of the refinement form
+    SideArrays pside[6]{}, sside[6]{};
+    Hier<double> HP, HS;
+    Hier<float> HP32, HS32;
+    ProbParm hpp{};
+    ProbParm* dpp = nullptr;
+    unsigned long long* dscal = nullptr;
+    unsigned long long* hscal = nullptr;
+    double time = 0.0;
+    int step = 0;
+    int eidx = E_ID;
+    int bg[NUM_SPECIES] = {};
+    int pbct[6] = {}, ebct[6] = {}, eebct[6] = {}, ibct[6] = {}, nbct[6] = {};
+    std::string err;
+    Prof prof;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // last-solve bookkeeping
+    long long poisson_iters = 0, species_iters = 0;
+    int not_converged = 0;
+    double max_poisson_res = 0.0;
+};
+
+std::string g_create_err;
+
+void set_err(Ctx* c, const std::string& m)
+{
+    if (c)
+        c->err = m;
+    else
+        g_create_err = m;
+}
+
+void make_bct(const Ctx& c, const int* lo, const int* hi, int* out)
+{
+    for (int d = 0; d < 3; ++d)
+    {
+        if (d >= c.cfg.dim || c.cfg.is_periodic[d])
+        {
+            out[d] = MG_PER;
+            out[d + 3] = MG_PER;
+        } else
+        {
+            out[d] = mg_type(lo[d]);
+            out[d + 3] = mg_type(hi[d]);
+        }
+    }
+}
+
+const int* bct_for(const Ctx& c, int comp)
+{
+    if (comp == c.eidx) return c.ebct;
+    if (comp == EEN_ID) return c.eebct;
+    return plasmachem::get_charge(comp) != 0 ? c.ibct : c.nbct;
+}
+const int* bclo_for(const Ctx& c, int comp)
+{
+    if (comp == c.eidx) return c.cfg.eden_bc_lo;
+    if (comp == EEN_ID) return c.cfg.eenrg_bc_lo;
+    return plasmachem::get_charge(comp) != 0 ? c.cfg.ion_bc_lo : c.cfg.neutral_bc_lo;
+}
+const int* bchi_for(const Ctx& c, int comp)
+{
+    if (comp == c.eidx) return c.cfg.eden_bc_hi;
+    if (comp == EEN_ID) return c.cfg.eenrg_bc_hi;
+    return plasmachem::get_charge(comp) != 0 ? c.cfg.ion_bc_hi : c.cfg.neutral_bc_hi;
+}
+
+double applied_potential(const vd_config& cfg, double t, int domend, int d)
+{
+    // Source/HelperFuncs.H:125-161
+    const double amp = (domend == -1) ? cfg.voltage_amp_lo[d] : cfg.voltage_amp_hi[d];
+    if (cfg.voltage_profile == 1) return std::sin(2.0 * PI * cfg.voltage_freq * t) * amp;
+    if (cfg.voltage_profile == 2)
+    {
+        const double vc = cfg.voltage_center, vd_ = cfg.voltage_dur;
+        if (t <= vc) return (vc - t < vd_ / 2.0) ? (1.0 - (vc - t) / (vd_ / 2.0)) * amp : 0.0;
+        return (t - vc < vd_ / 2.0) ? (1.0 - (t - vc) / (vd_ / 2.0)) * amp : 0.0;
+    }
+    return amp;
+}
+
+double read_norm(Ctx& c)
+{
+    VD_CUDA_OK(cudaMemcpyAsync(c.hscal, c.dscal, sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, c.st));
+    VD_CUDA_OK(cudaStreamSynchronize(c.st));
+    double v;
+    std::memcpy(&v, c.hscal, sizeof(double));
+    return v;
+}
+
+template <typename T>
+double resid_norm(Ctx& c, const MGOp<T>& op, const T* x, const T* f, T* rout, bool inh,
+                  double* fnorm = nullptr)
+{
+    VD_CUDA_OK(cudaMemsetAsync(c.dscal, 0, 2 * sizeof(unsigned long long), c.st));
+    LAUNCH(k_mg_resid_norm<T>, gsz(op.g.ncell()), BS, c.st, op, x, f, rout, c.dscal,
+           inh ? 1 : 0, fnorm ? 1 : 0);
+    if (fnorm)
+    {
+        VD_CUDA_OK(cudaMemcpyAsync(c.hscal + 1, c.dscal + 1, sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToHost, c.st));
+    }
+    const double r = read_norm(c);
+    if (fnorm) std::memcpy(fnorm, c.hscal + 1, sizeof(double));
+    return r;
+}
+
+// Boundary data of one solve: hook kernel + conversion to ghost form.
+void fill_bc(Ctx& c, int kind, int comp, const int* bct, int maxorder, double scale,
+             double time, SideArrays* sides)
+{
+    for (int s = 0; s < 6; ++s)
+    {
+        const int d = s % 3;
+        if (bct[s] == MG_PER) continue;
+        const int np = plane_count(c.g, d);
+        const int sgn = (s / 3) ? 1 : -1;
+        const double app = (kind == 0) ? applied_potential(c.cfg, time, sgn, d) : 0.0;
+        const int udef = (kind == 0) ? c.cfg.user_defined_potential : c.cfg.user_defined_species;
+        LAUNCH(k_bc_hook, gsz(np), BS, c.st, c.G, s, kind, comp, c.S, sides[s], time, app, udef,
+               c.cfg.gas_temperature, c.cfg.gas_pressure, c.dpp);
+        LAUNCH(k_bc_finalize, gsz(np), BS, c.st, np, bct[s], c.g.n[d], maxorder, c.G.dx[d],
+               scale, sides[s]);
+    }
+}
+
+// Level-0 boundary arrays of an FP64 hierarchy point at the side arrays;
+// an FP32 hierarchy gets converted copies.
+void bind_sides64(Hier<double>& H, SideArrays* sides)
+{
+    for (int s = 0; s < 6; ++s)
+    {
+        H.g0[s] = sides[s].g;
+        H.c0[0][s] = sides[s].c0;
+        H.ra[0][s] = sides[s].ra;
+        H.rb[0][s] = sides[s].rb;
+    }
+}
+
+void bind_sides32(Ctx& c, Hier<float>& H, SideArrays* sides, const int* bct)
+{
+    for (int s = 0; s < 6; ++s)
+    {
+        if (bct[s] != MG_ROBIN) continue;
+        const int np = plane_count(c.g, s % 3);
+        LAUNCH((k_convert<float, double>), gsz(np), BS, c.st, H.c0[0][s], sides[s].c0, 1.0, np);
+        LAUNCH((k_convert<float, double>), gsz(np), BS, c.st, H.ra[0][s], sides[s].ra, 1.0, np);
+        LAUNCH((k_convert<float, double>), gsz(np), BS, c.st, H.rb[0][s], sides[s].rb, 1.0, np);
+    }
+}
+
+// Solve L(sol) = rhs on the fine level.  Plain: FP64 V-cycles smoothing the
+// solution.  Refined: FP64 residual, FP32 V-cycles on the normalised
+// correction, FP64 update; both stop on |r|_inf <= max(abs, rel |r0|_inf).
+int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* rhs,
+             vd_solve_stats* stats)
+{
+    const vd_config& cfg = c.cfg;
+    double b0 = 0.0;
+    const double r0 = resid_norm(c, H64.op[0], sol, rhs, (double*)nullptr, true, &b0);
+    // relative to the larger of |rhs| and |r0| (MLMG's "bnorm"/"resid0")
+    const double target =
+        std::max(cfg.linsolve_abstol, std::max(cfg.linsolve_reltol, 1e-16) * std::max(b0, r0));
+    vd_solve_stats st{};
+    st.initial_residual = r0;
+    st.final_residual = r0;
+    st.converged = 1;
+    if (r0 > target)
+    {
+        st.converged = 0;
+        if (cfg.mg_precision == VD_MG_FP32_REFINED)
+        {
+            const long long n = c.N;
+            double rn = r0;
+            // r64 holds f - L(sol)
+            resid_norm(c, H64.op[0], sol, rhs, c.r64, true);
+            const int inner = std::max(1, cfg.mg_inner_cycles);
+            while (st.iterations < cfg.linsolve_maxiter)
+            {
+                const double s = 1.0 / rn;
+                LAUNCH((k_convert<float, double>), gsz(n), BS, c.st, H32.f[0], c.r64, s, n);
+                LAUNCH(k_fill<float>, gsz(n), BS, c.st, H32.x[0], 0.0f, n);
+                for (int q = 0; q < inner; ++q)
+                {
+                    vcycle(H32, H32.x[0], H32.f[0], false, c.dscal, c.st);
+                    ++st.iterations;
+                }
+                LAUNCH(k_add_scaled<float>, gsz(n), BS, c.st, sol, H32.x[0], rn, n);
+                ++st.refinements;
+                rn = resid_norm(c, H64.op[0], sol, rhs, c.r64, true);
+                st.final_residual = rn;
+                if (rn <= target)
+                {
+                    st.converged = 1;
+                    break;
+                }
+            }
+        } else
+        {
+            for (int it = 1; it <= cfg.linsolve_maxiter; ++it)
+            {
+                vcycle(H64, sol, rhs, true, c.dscal, c.st);
+                st.iterations = it;
+                const double rn = resid_norm(c, H64.op[0], sol, rhs, (double*)nullptr, true);
+                st.final_residual = rn;
+                if (rn <= target)
+                {
+                    st.converged = 1;
+                    break;
+                }
+            }
+        }
+    }
+    if (stats) *stats = st;
+    if (!st.converged) c.not_converged++;
+    return st.iterations;
+}
+
+GradCtx grad_ctx(Ctx& c, Hier<double>& H, SideArrays* sides)
+{
+    GradCtx gc{};
+    gc.op = H.op[0];
+    for (int d = 0; d < 3; ++d) gc.dxi[d] = 1.0 / c.G.dx[d];
+    for (int s = 0; s < 6; ++s) gc.inneu_val[s] = sides[s].val;
+    return gc;
+}
+
+// ---- solve_potential (Source/PotentialSolve.cpp:19-554)
+void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats)
+{
+    const vd_config& cfg = c.cfg;
+    const double ps = cfg.potential_scale;
+    LAUNCH(k_poisson_rhs, gsz(c.N), BS, c.st, c.G, Sold, c.S, c.phi_rhs, c.phi_sol,
+           cfg.do_spacechrg, cfg.poisson_warm_start, ps, time, c.dpp);
+    fill_bc(c, 0, POT_ID, c.pbct, 2, 1.0 / ps, time, c.pside);
+    hier_set_ops(c.HP, 0.0, 1.0, -1.0, c.pbct, 2);
+    hier_coarsen_coeffs(c.HP, c.pbct, c.st);
+    if (cfg.mg_precision == VD_MG_FP32_REFINED)
+    {
+        bind_sides32(c, c.HP32, c.pside, c.pbct);
+        hier_set_ops(c.HP32, 0.0, 1.0, -1.0, c.pbct, 2);
+        hier_coarsen_coeffs(c.HP32, c.pbct, c.st);
+    }
+    for (int s = 0; s < 6; ++s)
+        if (c.pbct[s] == MG_INNEU)
+            LAUNCH(k_inneu_adjust, gsz(plane_count(c.g, s % 3)), BS, c.st, c.g, s,
+                   (const double*)nullptr, -1.0, 1.0, c.G.dx[s % 3], c.pside[s].val, c.phi_rhs);
+    vd_solve_stats st{};
+    const int it = mg_solve(c, c.HP, c.HP32, c.phi_sol, c.phi_rhs, &st);
+    c.poisson_iters += it;
+    c.max_poisson_res = std::max(c.max_poisson_res, st.final_residual);
+    if (stats) *stats = st;
+    LAUNCH(k_efield, gsz(c.N), BS, c.st, grad_ctx(c, c.HP, c.pside), c.phi_sol, c.S, ps);
+}
+
+// ---- explicit sources of every transported component
+void explicit_rhs(Ctx& c, double time)
+{
+    const vd_config& cfg = c.cfg;
+    ExplParams P{};
+    P.G = c.G;
+    P.S = c.S;
+    P.expl = c.expl;
+    P.rxn_een = cfg.elecenergy_solve ? c.rxn_een : nullptr;
+    P.Tg = cfg.gas_temperature;
+    P.Pg = cfg.gas_pressure;
+    P.time = time;
+    P.dt = cfg.dt;
+    P.dxmin = c.G.dx[0];
+    for (int d = 1; d < cfg.dim; ++d) P.dxmin = std::min(P.dxmin, c.G.dx[d]);
+    P.hyp_order = cfg.hyp_order;
+    P.weno_scheme = cfg.weno_scheme;
+    P.user_vel = cfg.user_defined_vel;
+    P.do_transport = cfg.do_transport;
+    P.do_reactions = cfg.do_reactions;
+    P.do_bg_rxn = cfg.do_bg_reactions;
+    P.pp = c.dpp;
+    int n = 0;
+    for (int sp = 0; sp < NUM_SPECIES; ++sp)
+    {
+        P.bg[sp] = c.bg[sp];
+        if (c.bg[sp]) continue;
+        P.comp[n] = sp;
+        for (int d = 0; d < 3; ++d)
+        {
+            P.bclo[n][d] = bclo_for(c, sp)[d];
+            P.bchi[n][d] = bchi_for(c, sp)[d];
+        }
+        ++n;
+    }
+    if (cfg.elecenergy_solve)
+    {
+        P.comp[n] = EEN_ID;
+        for (int d = 0; d < 3; ++d)
+        {
+            P.bclo[n][d] = cfg.eenrg_bc_lo[d];
+            P.bchi[n][d] = cfg.eenrg_bc_hi[d];
+        }
+        ++n;
+    }
+    P.ntr = n;
+    const bool prof = t_prof && t_prof->id == VD_PROF_EXPLICIT;
+    if (prof)
+    {
+        // inputs: every species, E (3), Te, reduced field (EEN too when it is
+        // transported); outputs: one source per non-background component
+        // (+ the energy-exchange term)
+        const int nin = NUM_SPECIES + 5 + (cfg.elecenergy_solve ? 1 : 0);
+        const int nout = NUM_SPECIES + (cfg.elecenergy_solve ? 2 : 0);
+        t_prof->bytes = 8.0 * (nin + nout) * (double)c.N;
+        t_prof->begin(c.st);
+    }
+    LAUNCH(k_explicit, gsz(c.N), BS, c.st, P);
+    if (prof) t_prof->end(c.st);
+}
+
+// ---- implicit_solve_scalar (Source/ScalarSolve.cpp:380-858)
+void species_solve(Ctx& c, int comp, double time, const double* Sold, vd_solve_stats* stats)
+{
+    const vd_config& cfg = c.cfg;
+    const double ts = cfg.time_scale;
+    const double scale = (comp == EEN_ID) ? cfg.elecenergy_scale : cfg.species_scale[comp];
+    const int* bct = bct_for(c, comp);
+    for (int d = 0; d < cfg.dim; ++d)
+        LAUNCH(k_species_faces, gsz(face_count(c.g, d)), BS, c.st, c.g, d, c.S, comp,
+               cfg.gas_temperature, c.HS.bf[0][d]);
+    LAUNCH(k_species_rhs, gsz(c.N), BS, c.st, c.g, c.S, Sold, c.expl, comp, cfg.dt, ts, scale,
+           c.spec_rhs, c.u[comp]);
+    fill_bc(c, 1, comp, bct, 3, 1.0 / scale, time, c.sside);
+    hier_set_ops(c.HS, (1.0 / cfg.dt) * ts * 1.0, ts, 1.0, bct, 3);
+    hier_coarsen_coeffs(c.HS, bct, c.st);
+    if (cfg.mg_precision == VD_MG_FP32_REFINED)
+    {
+        for (int d = 0; d < cfg.dim; ++d)
+        {
+            const long long nf = face_count(c.g, d);
+            LAUNCH((k_convert<float, double>), gsz(nf), BS, c.st, c.HS32.bf[0][d], c.HS.bf[0][d],
+                   1.0, nf);
+        }
+        bind_sides32(c, c.HS32, c.sside, bct);
+        hier_set_ops(c.HS32, (1.0 / cfg.dt) * ts * 1.0, ts, 1.0, bct, 3);
+        hier_coarsen_coeffs(c.HS32, bct, c.st);
+    }
+    for (int s = 0; s < 6; ++s)
+        if (bct[s] == MG_INNEU)
+            LAUNCH(k_inneu_adjust, gsz(plane_count(c.g, s % 3)), BS, c.st, c.g, s,
+                   (const double*)c.HS.bf[0][s % 3], 1.0, ts, c.G.dx[s % 3], c.sside[s].val,
+                   c.spec_rhs);
+    vd_solve_stats st{};
+    const int it = mg_solve(c, c.HS, c.HS32, c.u[comp], c.spec_rhs, &st);
+    c.species_iters += it;
+    if (stats) *stats = st;
+}
+
+void joule(Ctx& c)
+{
+    JouleParams P{};
+    P.pot = grad_ctx(c, c.HP, c.pside);
+    P.phi_sol = c.phi_sol;
+    P.ps = c.cfg.potential_scale;
+    P.ue = c.u[c.eidx];
+    P.escale = c.cfg.species_scale[c.eidx];
+    P.S = c.S;
+    P.expl = c.expl;
+    P.ejh = c.ejh;
+    for (int d = 0; d < 3; ++d) P.dx[d] = c.G.dx[d];
+    P.Tg = c.cfg.gas_temperature;
+    P.floor_jh = c.cfg.floor_jh;
+    P.eidx = c.eidx;
+    LAUNCH(k_joule, gsz(c.N), BS, c.st, P);
+}
+
+FinalParams final_params(Ctx& c)
+{
+    FinalParams P{};
+    P.g = c.g;
+    P.S = c.S;
+    P.bound_specden = c.cfg.bound_specden;
+    P.min_e = c.cfg.min_electron_density;
+    P.min_s = c.cfg.min_species_density;
+    P.min_te = c.cfg.min_electron_temp;
+    P.eidx = c.eidx;
+    P.Tg = c.cfg.gas_temperature;
+    P.ejh = c.ejh;
+    P.rxn_een = c.rxn_een;
+    P.expl = c.expl;
+    P.dt = c.cfg.dt;
+    for (int sp = 0; sp < NUM_SPECIES; ++sp) P.bg[sp] = c.bg[sp];
+    return P;
+}
+
+void add_solved(Ctx& c, FinalParams& P, int comp)
+{
+    P.comp[P.nsol] = comp;
+    P.u[P.nsol] = c.u[comp];
+    P.scale[P.nsol] = (comp == EEN_ID) ? c.cfg.elecenergy_scale : c.cfg.species_scale[comp];
+    P.nsol++;
+}
+
+// ---- one coarse step (Source/Evolve.cpp:136-617)
+void step_once(Ctx& c)
+{
+    const vd_config& cfg = c.cfg;
+    const double dt = cfg.dt;
+    const int ncorr = std::max(1, cfg.num_timestep_correctors);
+    const size_t bytes = sizeof(double) * (size_t)NVAR * c.N;
+    if (ncorr > 1) VD_CUDA_OK(cudaMemcpyAsync(c.Sold, c.S, bytes, cudaMemcpyDeviceToDevice, c.st));
+    const double* Sold = (ncorr > 1) ? c.Sold : c.S;
+    for (int niter = 0; niter < ncorr; ++niter)
+    {
+        const double t = c.time + ((niter > 0) ? 0.5 * dt : 0.0);
+        poisson(c, t, Sold, nullptr);
+        explicit_rhs(c, t);
+        FinalParams P = final_params(c);
+        species_solve(c, c.eidx, t, Sold, nullptr);
+        add_solved(c, P, c.eidx);
+        if (cfg.elecenergy_solve)
+        {
+            joule(c);
+            species_solve(c, EEN_ID, t, Sold, nullptr);
+            add_solved(c, P, EEN_ID);
+            P.een_solved = 1;
+            P.heat_diag = 1;
+        }
+        P.lfa = cfg.using_LFA;
+        for (int sp = 0; sp < NUM_SPECIES; ++sp)
+        {
+            if (c.bg[sp] || sp == c.eidx) continue;
+            species_solve(c, sp, t, Sold, nullptr);
+            add_solved(c, P, sp);
+        }
+        P.do_bg_rxn = cfg.do_bg_reactions;
+        LAUNCH(k_finalize, gsz(c.N), BS, c.st, P);
+        if (niter < ncorr - 1)
+            LAUNCH(k_midpoint, gsz((long long)NVAR * c.N), BS, c.st, c.S, c.Sold,
+                   (long long)NVAR * c.N);
+    }
+    c.time += dt;
+    c.step += 1;
+}
+
+__global__ void k_initdomain(Geo G, double* S, const ProbParm* pp)
+{
+    const long long N = G.g.ncell();
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        cell_of(G.g, t, i, j, k);
+        Array4 v = state_view(S, G.g);
+        v.clamp = 0;
+        GeometryData gd;
+        for (int d = 0; d < 3; ++d)
+        {
+            gd.prob_lo[d] = G.plo[d];
+            gd.prob_hi[d] = G.phi[d];
+            gd.dx[d] = G.dx[d];
+            gd.n_cell[d] = G.g.n[d];
+        }
+        Box bx{{i, j, k}, {i, j, k}};
+        initdomaindata(bx, v, gd, pp);
+    }
+}
+
+// ---------------------------------------------------------- config I/O
+struct Key
+{
+    const char* name;
+    int kind; // 0 int, 1 double, 2 int[3], 3 double[3]
+    size_t off;
+};
+
+#define KI(n, f) {n, 0, offsetof(vd_config, f)}
+#define KD(n, f) {n, 1, offsetof(vd_config, f)}
+#define KI3(n, f) {n, 2, offsetof(vd_config, f)}
+#define KD3(n, f) {n, 3, offsetof(vd_config, f)}
+
+const Key g_keys[] = {
+    KI3("amr.n_cell", n_cell), KD3("geometry.prob_lo", prob_lo), KD3("geometry.prob_hi", prob_hi),
+    KI3("geometry.is_periodic", is_periodic), KD("vidyut.dt", dt),
+    KI("vidyut.num_timestep_correctors", num_timestep_correctors),
+    KI("vidyut.hyp_order", hyp_order), KI("vidyut.weno_scheme", weno_scheme),
+    KI("vidyut.do_reactions", do_reactions), KI("vidyut.do_transport", do_transport),
+    KI("vidyut.do_spacechrg", do_spacechrg), KI("vidyut.elecenergy_solve", elecenergy_solve),
+    KI("vidyut.using_LFA", using_LFA), KI("vidyut.floor_jh", floor_jh),
+    KI("vidyut.bound_specden", bound_specden), KI("vidyut.do_bg_reactions", do_bg_reactions),
+    KI("vidyut.user_defined_potential", user_defined_potential),
+    KI("vidyut.user_defined_species", user_defined_species),
+    KI("vidyut.user_defined_vel", user_defined_vel),
+    KD("vidyut.min_species_density", min_species_density),
+    KD("vidyut.min_electron_density", min_electron_density),
+    KD("vidyut.min_electron_temp", min_electron_temp),
+    KD("vidyut.gas_temperature", gas_temperature), KD("vidyut.gas_pressure", gas_pressure),
+    KI3("vidyut.pot_bc_lo", pot_bc_lo), KI3("vidyut.pot_bc_hi", pot_bc_hi),
+    KI3("vidyut.eden_bc_lo", eden_bc_lo), KI3("vidyut.eden_bc_hi", eden_bc_hi),
+    KI3("vidyut.eenrg_bc_lo", eenrg_bc_lo), KI3("vidyut.eenrg_bc_hi", eenrg_bc_hi),
+    KI3("vidyut.ion_bc_lo", ion_bc_lo), KI3("vidyut.ion_bc_hi", ion_bc_hi),
+    KI3("vidyut.neutral_bc_lo", neutral_bc_lo), KI3("vidyut.neutral_bc_hi", neutral_bc_hi),
+    KI("vidyut.voltage_profile", voltage_profile),
+    KD3("vidyut.voltage_amp_lo", voltage_amp_lo), KD3("vidyut.voltage_amp_hi", voltage_amp_hi),
+    KD("vidyut.voltage_freq", voltage_freq), KD("vidyut.voltage_dur", voltage_dur),
+    KD("vidyut.voltage_center", voltage_center),
+    KD("vidyut.linsolve_reltol", linsolve_reltol), KD("vidyut.linsolve_abstol", linsolve_abstol),
+    KD("vidyut.linsolve_bot_reltol", linsolve_bot_reltol),
+    KD("vidyut.linsolve_bot_abstol", linsolve_bot_abstol),
+    KI("vidyut.linsolve_num_pre_smooth", linsolve_num_pre_smooth),
+    KI("vidyut.linsolve_num_post_smooth", linsolve_num_post_smooth),
+    KI("vidyut.linsolve_num_final_smooth", linsolve_num_final_smooth),
+    KI("vidyut.linsolve_num_bottom_smooth", linsolve_num_bottom_smooth),
+    KI("vidyut.linsolve_maxiter", linsolve_maxiter),
+    KI("vidyut.linsolve_max_coarsening_level", linsolve_max_coarsening_level),
+    KD("vidyut.potential_scale", potential_scale), KD("vidyut.elecenergy_scale", elecenergy_scale),
+    KD("vidyut.time_scale", time_scale), KI("vidyut.mg_precision", mg_precision),
+    KI("vidyut.mg_inner_cycles", mg_inner_cycles),
+    KI("vidyut.poisson_warm_start", poisson_warm_start), KI("vidyut.device", device),
+};
+
+} // namespace
+
+// ================================================================ C ABI
+extern "C" {
+
+vd_status vd_config_init(vd_config* c)
+{
+    if (!c) return VD_ERR_INVALID_ARG;
+    std::memset(c, 0, sizeof(*c));
+    c->dim = 3;
+    for (int d = 0; d < 3; ++d)
+    {
+        c->n_cell[d] = 32;
+        c->prob_hi[d] = 1.0;
+        c->pot_bc_lo[d] = c->pot_bc_hi[d] = HNEUBC;
+        c->eden_bc_lo[d] = c->eden_bc_hi[d] = HNEUBC;
+        c->eenrg_bc_lo[d] = c->eenrg_bc_hi[d] = HNEUBC;
+        c->ion_bc_lo[d] = c->ion_bc_hi[d] = HNEUBC;
+        c->neutral_bc_lo[d] = c->neutral_bc_hi[d] = HNEUBC;
+    }
+    c->dt = 1e-12;
+    c->num_timestep_correctors = 1;
+    c->hyp_order = 1;
+    c->weno_scheme = 3;
+    c->do_reactions = 1;
+    c->do_transport = 1;
+    c->do_spacechrg = 1;
+    c->min_species_density = 1e-20;
+    c->min_electron_density = 1e12;
+    c->min_electron_temp = 300.0;
+    c->gas_temperature = T_NTP;
+    c->gas_pressure = P_NTP;
+    c->voltage_freq = 1.0;
+    c->linsolve_reltol = 1e-10;
+    c->linsolve_abstol = 1e-10;
+    c->linsolve_bot_reltol = 1e-10;
+    c->linsolve_bot_abstol = -1.0;
+    c->linsolve_num_pre_smooth = 2;
+    c->linsolve_num_post_smooth = 2;
+    c->linsolve_num_final_smooth = 8;
+    c->linsolve_num_bottom_smooth = 0;
+    c->linsolve_maxiter = 100;
+    c->linsolve_max_coarsening_level = 10;
+    c->potential_scale = 1.0;
+    c->elecenergy_scale = 1.0;
+    c->time_scale = 1.0;
+    for (int i = 0; i < VD_MAX_SPECIES; ++i) c->species_scale[i] = 1.0;
+    c->mg_precision = VD_MG_FP64;
+    c->mg_inner_cycles = 2;
+    return VD_OK;
+}
+
+vd_status vd_config_set(vd_config* c, const char* key, const char* value)
+{
+    if (!c || !key || !value) return VD_ERR_INVALID_ARG;
+    const std::string k(key);
+    std::istringstream vs(value);
+    if (k == "dim")
+    {
+        vs >> c->dim;
+        return (c->dim == 2 || c->dim == 3) ? VD_OK : VD_ERR_INVALID_ARG;
+    }
+    if (k == "vidyut.bg_species_ids")
+    {
+        int v, n = 0;
+        while (vs >> v && n < VD_MAX_SPECIES) c->bg_species_ids[n++] = v;
+        c->num_bg_species = n;
+        return VD_OK;
+    }
+    if (k == "vidyut.scaling_species_ids" || k == "vidyut.scale_values")
+        return VD_ERR_UNSUPPORTED; // use vd_config.species_scale directly
+    for (const Key& e : g_keys)
+    {
+        if (k != e.name) continue;
+        char* base = reinterpret_cast<char*>(c) + e.off;
+        switch (e.kind)
+        {
+        case 0: vs >> *reinterpret_cast<int*>(base); break;
+        case 1: vs >> *reinterpret_cast<double*>(base); break;
+        case 2:
+            for (int d = 0; d < 3 && (vs >> reinterpret_cast<int*>(base)[d]); ++d) {}
+            break;
+        case 3:
+            for (int d = 0; d < 3 && (vs >> reinterpret_cast<double*>(base)[d]); ++d) {}
+            break;
+        }
+        return vs.fail() && !vs.eof() ? VD_ERR_INVALID_ARG : VD_OK;
+    }
+    return VD_ERR_INVALID_ARG;
+}
+
+vd_status vd_case_info(vd_case_info_t* info)
+{
+    if (!info) return VD_ERR_INVALID_ARG;
+    std::memset(info, 0, sizeof(*info));
+    info->num_species = NUM_SPECIES;
+    info->nvar = NVAR;
+    info->e_id = E_ID;
+    info->een_id = EEN_ID;
+    info->etemp_id = ETEMP_ID;
+    info->pot_id = POT_ID;
+    info->efx_id = EFX_ID;
+    info->ref_id = REF_ID;
+    info->ejh_id = EJH_ID;
+    info->eih_id = EIH_ID;
+    info->cmask_id = CMASK_ID;
+    int q[NUM_SPECIES];
+    CKCHRG(q);
+    std::vector<std::string> names;
+    CKSYMS_STR(names);
+    for (int s = 0; s < NUM_SPECIES && s < VD_MAX_SPECIES; ++s)
+    {
+        info->charge[s] = q[s];
+        if (s < (int)names.size()) std::strncpy(info->names[s], names[s].c_str(), 15);
+    }
+#ifdef VD_CASE_NAME
+    std::strncpy(info->case_name, VD_CASE_NAME, 63);
+#endif
+    return VD_OK;
+}
+
+vd_status vd_create(const vd_config* cfg, void** out)
+{
+    if (!cfg || !out) return VD_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (cfg->dim != 2 && cfg->dim != 3)
+    {
+        g_create_err = "dim must be 2 or 3";
+        return VD_ERR_INVALID_ARG;
+    }
+    if (cfg->hyp_order != 1 && cfg->hyp_order != 2 && cfg->hyp_order != 5)
+    {
+        g_create_err = "hyp_order must be 1, 2 or 5 (Source/Vidyut.cpp:448-461)";
+        return VD_ERR_INVALID_ARG;
+    }
+    if (cfg->weno_scheme < 1 || cfg->weno_scheme > 3)
+    {
+        g_create_err = "weno_scheme must be 1, 2 or 3";
+        return VD_ERR_INVALID_ARG;
+    }
+#ifndef VD_HAS_USER_TRANSPORT
+    if (cfg->user_defined_potential || cfg->user_defined_species || cfg->user_defined_vel)
+    {
+        g_create_err = "this case defines no user_transport hooks";
+        return VD_ERR_UNSUPPORTED;
+    }
+#endif
+    for (int d = 0; d < cfg->dim; ++d)
+        if (cfg->n_cell[d] < 1 || !(cfg->prob_hi[d] > cfg->prob_lo[d]))
+        {
+            g_create_err = "bad grid";
+            return VD_ERR_INVALID_ARG;
+        }
+    Ctx* c = new Ctx();
+    try
+    {
+        c->cfg = *cfg;
+        c->dev = cfg->device;
+        VD_CUDA_OK(cudaSetDevice(c->dev));
+        VD_CUDA_OK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+        GridDev& g = c->g;
+        g.dim = cfg->dim;
+        for (int d = 0; d < 3; ++d)
+        {
+            const bool act = d < cfg->dim;
+            g.n[d] = act ? cfg->n_cell[d] : 1;
+            g.per[d] = act ? cfg->is_periodic[d] : 0;
+            c->G.plo[d] = act ? cfg->prob_lo[d] : 0.0;
+            c->G.phi[d] = act ? cfg->prob_hi[d] : 1.0;
+            c->G.dx[d] = act ? (cfg->prob_hi[d] - cfg->prob_lo[d]) / cfg->n_cell[d] : 1.0;
+        }
+        c->G.g = g;
+        c->N = g.ncell();
+        for (int i = 0; i < cfg->num_bg_species; ++i)
+        {
+            const int b = cfg->bg_species_ids[i];
+            if (b < 0 || b >= NUM_SPECIES) throw CudaError("bg_species_ids out of range");
+            c->bg[b] = 1;
+        }
+        make_bct(*c, cfg->pot_bc_lo, cfg->pot_bc_hi, c->pbct);
+        make_bct(*c, cfg->eden_bc_lo, cfg->eden_bc_hi, c->ebct);
+        make_bct(*c, cfg->eenrg_bc_lo, cfg->eenrg_bc_hi, c->eebct);
+        make_bct(*c, cfg->ion_bc_lo, cfg->ion_bc_hi, c->ibct);
+        make_bct(*c, cfg->neutral_bc_lo, cfg->neutral_bc_hi, c->nbct);
+
+        const long long N = c->N;
+        c->S = c->A.get<double>((size_t)NVAR * N);
+        VD_CUDA_OK(cudaMemset(c->S, 0, sizeof(double) * (size_t)NVAR * N));
+        c->Sold = (cfg->num_timestep_correctors > 1) ? c->A.get<double>((size_t)NVAR * N) : c->S;
+        c->expl = c->A.get<double>((size_t)VD_NT * N);
+        VD_CUDA_OK(cudaMemset(c->expl, 0, sizeof(double) * (size_t)VD_NT * N));
+        c->rxn_een = c->A.get<double>(N);
+        c->ejh = c->A.get<double>(N);
+        for (int sp = 0; sp < NUM_SPECIES; ++sp)
+            if (!c->bg[sp]) c->u[sp] = c->A.get<double>(N);
+        c->u[EEN_ID] = c->A.get<double>(N);
+        c->phi_sol = c->A.get<double>(N);
+        c->phi_rhs = c->A.get<double>(N);
+        c->spec_rhs = c->A.get<double>(N);
+        for (int s = 0; s < 6; ++s)
+        {
+            const int np = plane_count(g, s % 3);
+            for (SideArrays* sa : {&c->pside[s], &c->sside[s]})
+            {
+                sa->val = c->A.get<double>(np);
+                sa->ra = c->A.get<double>(np);
+                sa->rb = c->A.get<double>(np);
+                sa->rf = c->A.get<double>(np);
+                sa->g = c->A.get<double>(np);
+                sa->c0 = c->A.get<double>(np);
+            }
+        }
+        const double dx[3] = {c->G.dx[0], c->G.dx[1], c->G.dx[2]};
+        const int mcl = cfg->linsolve_max_coarsening_level;
+        hier_build(c->HP, c->A, g, dx, mcl, false, false);
+        hier_build(c->HS, c->A, g, dx, mcl, true, false);
+        // the FP64 species hierarchy's level-0 faces are written by the set-up
+        // kernels; boundary arrays of both FP64 hierarchies alias the side arrays
+        bind_sides64(c->HP, c->pside);
+        bind_sides64(c->HS, c->sside);
+        if (cfg->mg_precision == VD_MG_FP32_REFINED)
+        {
+            hier_build(c->HP32, c->A, g, dx, mcl, false, true);
+            hier_build(c->HS32, c->A, g, dx, mcl, true, true);
+            c->r64 = c->A.get<double>(N);
+        }
+        for (Hier<double>* h : {&c->HP, &c->HS})
+        {
+            h->nu1 = cfg->linsolve_num_pre_smooth;
+            h->nu2 = cfg->linsolve_num_post_smooth;
+        }
+        for (Hier<float>* h : {&c->HP32, &c->HS32})
+        {
+            h->nu1 = cfg->linsolve_num_pre_smooth;
+            h->nu2 = cfg->linsolve_num_post_smooth;
+        }
+        c->HP.prof_tag = VD_PROF_POISSON_SMOOTH;
+        c->HP32.prof_tag = VD_PROF_POISSON_SMOOTH32;
+        VD_CUDA_OK(cudaEventCreate(&c->ev0));
+        VD_CUDA_OK(cudaEventCreate(&c->ev1));
+        c->dpp = c->A.get<ProbParm>(1);
+        VD_CUDA_OK(cudaMemcpy(c->dpp, &c->hpp, sizeof(ProbParm), cudaMemcpyHostToDevice));
+        c->dscal = c->A.get<unsigned long long>(2);
+        VD_CUDA_OK(cudaMallocHost(&c->hscal, 2 * sizeof(unsigned long long)));
+        // electron index (Source/Vidyut.cpp:132-144)
+        c->eidx = E_ID;
+        VD_CUDA_OK(cudaDeviceSynchronize());
+    } catch (const CudaError& e)
+    {
+        g_create_err = e.msg;
+        c->A.release();
+        delete c;
+        return VD_ERR_CUDA;
+    }
+    *out = c;
+    return VD_OK;
+}
+
+vd_status vd_destroy(void* ctx)
+{
+    if (!ctx) return VD_ERR_INVALID_ARG;
+    Ctx* c = static_cast<Ctx*>(ctx);
+    cudaSetDevice(c->dev);
+    cudaStreamSynchronize(c->st);
+    c->A.release();
+    for (auto e : c->prof.a) cudaEventDestroy(e);
+    for (auto e : c->prof.b) cudaEventDestroy(e);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->hscal) cudaFreeHost(c->hscal);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+    return VD_OK;
+}
+
+#define VD_TRY(body)                                                             \
+    if (!ctx) return VD_ERR_INVALID_ARG;                                         \
+    Ctx* c = static_cast<Ctx*>(ctx);                                             \
+    t_prof = &c->prof;                                                           \
+    try                                                                          \
+    {                                                                            \
+        VD_CUDA_OK(cudaSetDevice(c->dev));                                       \
+        body;                                                                    \
+        VD_CUDA_OK(cudaStreamSynchronize(c->st));                                \
+    } catch (const CudaError& e)                                                 \
+    {                                                                            \
+        c->err = e.msg;                                                          \
+        return VD_ERR_CUDA;                                                      \
+    }
+
+vd_status vd_init_domain(void* ctx, const char* prob_inputs)
+{
+    VD_TRY({
+        auto table = vd::ParmParse::parse(prob_inputs ? prob_inputs : "");
+        vd::ParmParse pp(&table, "prob");
+        c->hpp = ProbParm{};
+        amrex_probinit(c->hpp, pp);
+        VD_CUDA_OK(cudaMemcpyAsync(c->dpp, &c->hpp, sizeof(ProbParm), cudaMemcpyHostToDevice, c->st));
+        LAUNCH(k_initdomain, gsz(c->N), BS, c->st, c->G, c->S, c->dpp);
+        c->time = 0.0;
+        c->step = 0;
+    });
+    return VD_OK;
+}
+
+vd_status vd_set_state(void* ctx, int comp, int ncomp, const double* src, int on_device)
+{
+    if (!ctx || !src || comp < 0 || ncomp < 1 || comp + ncomp > NVAR) return VD_ERR_INVALID_ARG;
+    VD_TRY({
+        VD_CUDA_OK(cudaMemcpyAsync(c->S + (size_t)comp * c->N, src,
+                                   sizeof(double) * (size_t)ncomp * c->N,
+                                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                   c->st));
+    });
+    return VD_OK;
+}
+
+vd_status vd_get_state(void* ctx, int comp, int ncomp, double* dst, int on_device)
+{
+    if (!ctx || !dst || comp < 0 || ncomp < 1 || comp + ncomp > NVAR) return VD_ERR_INVALID_ARG;
+    VD_TRY({
+        VD_CUDA_OK(cudaMemcpyAsync(dst, c->S + (size_t)comp * c->N,
+                                   sizeof(double) * (size_t)ncomp * c->N,
+                                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                   c->st));
+    });
+    return VD_OK;
+}
+
+vd_status vd_set_time(void* ctx, double time, int step)
+{
+    if (!ctx) return VD_ERR_INVALID_ARG;
+    Ctx* c = static_cast<Ctx*>(ctx);
+    c->time = time;
+    c->step = step;
+    return VD_OK;
+}
+
+vd_status vd_get_time(void* ctx, double* time, int* step)
+{
+    if (!ctx) return VD_ERR_INVALID_ARG;
+    Ctx* c = static_cast<Ctx*>(ctx);
+    if (time) *time = c->time;
+    if (step) *step = c->step;
+    return VD_OK;
+}
+
+vd_status vd_step(void* ctx, int nsteps, vd_step_stats* stats)
+{
+    if (nsteps < 0) return VD_ERR_INVALID_ARG;
+    VD_TRY({
+        c->poisson_iters = 0;
+        c->species_iters = 0;
+        c->not_converged = 0;
+        c->max_poisson_res = 0.0;
+        VD_CUDA_OK(cudaEventRecord(c->ev0, c->st));
+        for (int s = 0; s < nsteps; ++s) step_once(*c);
+        VD_CUDA_OK(cudaEventRecord(c->ev1, c->st));
+        VD_CUDA_OK(cudaEventSynchronize(c->ev1));
+        float ms = 0.f;
+        VD_CUDA_OK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        if (stats)
+        {
+            std::memset(stats, 0, sizeof(*stats));
+            stats->steps = nsteps;
+            stats->poisson_iterations = (int)c->poisson_iters;
+            stats->species_iterations = (int)c->species_iters;
+            stats->not_converged = c->not_converged;
+            stats->max_poisson_final_residual = c->max_poisson_res;
+            stats->time = c->time;
+            stats->gpu_ms = ms;
+        }
+    });
+    return c->not_converged ? VD_ERR_NOT_CONVERGED : VD_OK;
+}
+
+vd_status vd_profile_kernel(void* ctx, int kernel_id)
+{
+    VD_TRY({
+        c->prof.id = kernel_id;
+        c->prof.n = 0;
+        c->prof.bytes = 0.0;
+    });
+    return VD_OK;
+}
+
+vd_status vd_profile_read(void* ctx, long long* launches, double* total_ms,
+                          double* bytes_per_launch)
+{
+    double tot = 0.0;
+    VD_TRY({
+        for (int i = 0; i < c->prof.n; ++i)
+        {
+            float ms = 0.f;
+            VD_CUDA_OK(cudaEventSynchronize(c->prof.b[i]));
+            VD_CUDA_OK(cudaEventElapsedTime(&ms, c->prof.a[i], c->prof.b[i]));
+            tot += ms;
+        }
+    });
+    if (launches) *launches = c->prof.n;
+    if (total_ms) *total_ms = tot;
+    if (bytes_per_launch) *bytes_per_launch = c->prof.bytes;
+    return VD_OK;
+}
+
+vd_status vd_poisson_solve(void* ctx, double time, vd_solve_stats* stats)
+{
+    VD_TRY({
+        c->not_converged = 0;
+        poisson(*c, time, c->S, stats);
+    });
+    return c->not_converged ? VD_ERR_NOT_CONVERGED : VD_OK;
+}
+
+vd_status vd_explicit_rhs(void* ctx, double time, double* out, int on_device)
+{
+    VD_TRY({
+        explicit_rhs(*c, time);
+        if (out)
+            VD_CUDA_OK(cudaMemcpyAsync(out, c->expl, sizeof(double) * (size_t)VD_NT * c->N,
+                                       on_device ? cudaMemcpyDeviceToDevice
+                                                 : cudaMemcpyDeviceToHost,
+                                       c->st));
+    });
+    return VD_OK;
+}
+
+vd_status vd_implicit_diffusion(void* ctx, int spec, double time, const double* expl_in,
+                                int on_device, vd_solve_stats* stats)
+{
+    if (!ctx || !expl_in || spec < 0 || spec > NUM_SPECIES) return VD_ERR_INVALID_ARG;
+    VD_TRY({
+        c->not_converged = 0;
+        VD_CUDA_OK(cudaMemcpyAsync(c->expl, expl_in, sizeof(double) * (size_t)VD_NT * c->N,
+                                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                   c->st));
+        species_solve(*c, spec, time, c->S, stats);
+        FinalParams P = final_params(*c);
+        add_solved(*c, P, spec);
+        P.een_solved = (spec == EEN_ID) ? 1 : 0;
+        LAUNCH(k_finalize, gsz(c->N), BS, c->st, P);
+    });
+    return c->not_converged ? VD_ERR_NOT_CONVERGED : VD_OK;
+}
+
+vd_status vd_check_state(void* ctx, long long* nonfinite)
+{
+    if (!nonfinite) return VD_ERR_INVALID_ARG;
+    VD_TRY({
+        VD_CUDA_OK(cudaMemsetAsync(c->dscal, 0, sizeof(unsigned long long), c->st));
+        LAUNCH(k_nonfinite, gsz((long long)(NUM_SPECIES + 3) * c->N), BS, c->st, c->S,
+               (long long)(NUM_SPECIES + 3) * c->N, c->dscal);
+        VD_CUDA_OK(cudaMemcpyAsync(c->hscal, c->dscal, sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToHost, c->st));
+    });
+    *nonfinite = (long long)*c->hscal;
+    return *nonfinite ? VD_ERR_NONFINITE : VD_OK;
+}
+
+vd_status vd_launch_count(void* ctx, long long* launches)
+{
+    if (!launches) return VD_ERR_INVALID_ARG;
+    *launches = vd::g_launches;
+    return VD_OK;
+}
+
+vd_status vd_last_error(void* ctx, char* buf, int len)
+{
+    if (!buf || len < 1) return VD_ERR_INVALID_ARG;
+    const std::string& m = ctx ? static_cast<Ctx*>(ctx)->err : g_create_err;
+    std::strncpy(buf, m.c_str(), len - 1);
+    buf[len - 1] = 0;
+    return VD_OK;
+}
+
+} // extern "C"
