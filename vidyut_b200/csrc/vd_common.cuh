@@ -23,19 +23,27 @@ struct CudaError
 };
 
 // Grid of one multigrid level (or of the state): cell counts, active
-// dimension count, periodicity.  Index (i,j,k) -> i + nx*(j + ny*k).
+// dimension count, periodicity, storage layout.
+//   natural (rb = 0): (i,j,k) -> i + nx*(j + ny*k)            (the state)
+//   red-black split (rb = 1, nx even): the cells with (i+j+k) even come
+//   first, then the odd ones, each half in natural order of (i/2, j, k):
+//   (i,j,k) -> ((i+j+k)&1) * ncell/2 + (i>>1) + (nx/2)*(j + ny*k)
+// so one Gauss-Seidel colour is a contiguous, unit-stride array.
 struct GridDev
 {
     int n[3];
     int dim;
     int per[3];
+    int rb;
     __host__ __device__ long long ncell() const
     {
         return (long long)n[0] * n[1] * n[2];
     }
     __host__ __device__ long long idx(int i, int j, int k) const
     {
-        return i + (long long)n[0] * (j + (long long)n[1] * k);
+        const long long row = j + (long long)n[1] * k;
+        if (!rb) return i + (long long)n[0] * row;
+        return (long long)((i + j + k) & 1) * (ncell() >> 1) + (i >> 1) + (long long)(n[0] >> 1) * row;
     }
 };
 

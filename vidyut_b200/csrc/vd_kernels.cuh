@@ -93,7 +93,7 @@ __device__ __forceinline__ GpuArray<Real, 3> ga3(const double* v)
 }
 
 // ---------------- Poisson right-hand side (Source/PotentialSolve.cpp:252-277, :484)
-__global__ void k_poisson_rhs(Geo G, const double* __restrict__ Sold, double* Sv,
+__global__ void k_poisson_rhs(Geo G, GridDev gm, const double* __restrict__ Sold, double* Sv,
                               double* __restrict__ rhs, double* __restrict__ sol,
                               int do_spacechrg, int warm, double ps, double time,
                               const ProbParm* pp)
@@ -102,6 +102,9 @@ __global__ void k_poisson_rhs(Geo G, const double* __restrict__ Sold, double* Sv
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
          t += (long long)gridDim.x * blockDim.x)
     {
+        int ci, cj, ck;
+        cell_of(G.g, t, ci, cj, ck);
+        const long long m = gm.idx(ci, cj, ck);
         double r = 0.0;
         if (do_spacechrg)
         {
@@ -113,16 +116,14 @@ __global__ void k_poisson_rhs(Geo G, const double* __restrict__ Sold, double* Sv
             }
             r *= (-ECHARGE / EPS0);
 #ifndef VD_NO_USER_POTENTIAL_SOURCES
-            int i, j, k;
-            cell_of(G.g, t, i, j, k);
             Array4 sv = state_view(const_cast<double*>(Sold), G.g);
-            Array4 rv = cell_view(&r, i, j, k);
-            user_sources::add_user_potential_sources(i, j, k, sv, rv, ga3(G.plo), ga3(G.phi),
+            Array4 rv = cell_view(&r, ci, cj, ck);
+            user_sources::add_user_potential_sources(ci, cj, ck, sv, rv, ga3(G.plo), ga3(G.phi),
                                                      ga3(G.dx), time, *pp);
 #endif
         }
-        rhs[t] = r * (1.0 / ps);
-        sol[t] = warm ? Sv[POT_ID * N + t] / ps : 0.0;
+        rhs[m] = r * (1.0 / ps);
+        sol[m] = warm ? Sv[POT_ID * N + t] / ps : 0.0;
     }
 }
 
@@ -275,8 +276,13 @@ __device__ __forceinline__ double grad_at_face(const GradCtx& C, const double* _
     const int s = d + (lo ? 0 : 3);
     if (C.op.bct[s] == MG_INNEU) return C.inneu_val[s][plane_index(g, d, in[0], in[1], in[2])];
     const double x0 = x[g.idx(in[0], in[1], in[2])];
-    double cf;
-    const double gh = mg_nbr(C.op, x, in[0], in[1], in[2], d, lo ? -1 : 1, true, x0, cf);
+    double cf, gh;
+    if (d == 0)
+        gh = mg_nbr<0>(C.op, x, in[0], in[1], in[2], lo ? -1 : 1, true, x0, cf);
+    else if (d == 1)
+        gh = mg_nbr<1>(C.op, x, in[0], in[1], in[2], lo ? -1 : 1, true, x0, cf);
+    else
+        gh = mg_nbr<2>(C.op, x, in[0], in[1], in[2], lo ? -1 : 1, true, x0, cf);
     return lo ? (x0 - gh) * C.dxi[d] : (gh - x0) * C.dxi[d];
 }
 
@@ -290,7 +296,9 @@ __global__ void k_efield(GradCtx C, const double* __restrict__ sol, double* __re
          t += (long long)gridDim.x * blockDim.x)
     {
         int i, j, k;
-        cell_of(g, t, i, j, k);
+        i = (int)(t % g.n[0]);
+        j = (int)((t / g.n[0]) % g.n[1]);
+        k = (int)(t / ((long long)g.n[0] * g.n[1]));
         double E[3] = {0.0, 0.0, 0.0};
         for (int d = 0; d < g.dim; ++d)
         {
@@ -307,7 +315,7 @@ __global__ void k_efield(GradCtx C, const double* __restrict__ sol, double* __re
         nd = nd - S[E_ID * N + t];
         for (int d = 0; d < g.dim; ++d) Esum += E[d] * E[d];
         S[REF_ID * N + t] = (sqrt(Esum) / nd) / 1.0e-21;
-        S[POT_ID * N + t] = sol[t] * ps;
+        S[POT_ID * N + t] = sol[g.idx(i, j, k)] * ps;
     }
 }
 
@@ -474,7 +482,7 @@ __global__ void k_species_faces(GridDev g, int d, const double* __restrict__ S, 
     }
 }
 
-__global__ void k_species_rhs(GridDev g, const double* __restrict__ S,
+__global__ void k_species_rhs(GridDev g, GridDev gm, const double* __restrict__ S,
                               const double* __restrict__ Sold, const double* __restrict__ expl,
                               int spec, double dt, double ts, double scale,
                               double* __restrict__ rhs, double* __restrict__ sol)
@@ -483,9 +491,12 @@ __global__ void k_species_rhs(GridDev g, const double* __restrict__ S,
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
          t += (long long)gridDim.x * blockDim.x)
     {
+        int i, j, k;
+        cell_of(g, t, i, j, k);
+        const long long m = gm.idx(i, j, k);
         const double r = (1.0 / dt) * Sold[spec * N + t] + 1.0 * expl[spec * N + t];
-        rhs[t] = r * (ts / scale);
-        sol[t] = S[spec * N + t] * (1.0 / scale);
+        rhs[m] = r * (ts / scale);
+        sol[m] = S[spec * N + t] * (1.0 / scale);
     }
 }
 
@@ -496,6 +507,7 @@ struct JouleParams
     const double* phi_sol; // scaled Poisson solution
     double ps;
     const double* ue;      // electron solution (scaled, before the floor)
+    GridDev gm;            // layout of ue
     double escale;
     const double* S;
     double* expl;
@@ -580,7 +592,9 @@ __global__ void k_joule(JouleParams P)
                     gn = onesided_grad(S, g, N, P.eidx, face, sgn, d, P.dx[d]);
                 } else
                 {
-                    gn = (P.ue[qr] - P.ue[ql]) * (1.0 / P.dx[d]) * P.escale;
+                    gn = (P.ue[P.gm.idx(face[0], face[1], face[2])] -
+                          P.ue[P.gm.idx(lc[0], lc[1], lc[2])]) *
+                         (1.0 / P.dx[d]) * P.escale;
                 }
                 const double cd = charge * (mu * ne * ef - dc * gn);
                 jh += cd * ef;
@@ -616,6 +630,7 @@ struct FinalParams
     int bg[NUM_SPECIES];
     int do_bg_rxn;
     double dt;
+    GridDev gm; // layout of the solve outputs u[]
 };
 
 __global__ void k_finalize(FinalParams P)
@@ -625,6 +640,9 @@ __global__ void k_finalize(FinalParams P)
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
          t += (long long)gridDim.x * blockDim.x)
     {
+        int ci, cj, ck;
+        cell_of(P.g, t, ci, cj, ck);
+        const long long m = P.gm.idx(ci, cj, ck);
         // values of the iteration's starting state read before any write
         double spec_old[NUM_SPECIES];
 #pragma unroll
@@ -634,7 +652,7 @@ __global__ void k_finalize(FinalParams P)
         for (int q = 0; q < P.nsol; ++q)
         {
             const int c = P.comp[q];
-            double v = P.u[q][t] * P.scale[q];
+            double v = P.u[q][m] * P.scale[q];
             if (P.bound_specden && c != EEN_ID)
             {
                 if (c == P.eidx)
@@ -692,6 +710,14 @@ __global__ void k_nonfinite(const double* __restrict__ S, long long n, unsigned 
          t += (long long)gridDim.x * blockDim.x)
         if (!isfinite(S[t])) ++c;
     if (c) atomicAdd(cnt, c);
+}
+
+template <typename T>
+__global__ void k_add_same(T* __restrict__ x, const T* __restrict__ e, long long n)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        x[t] += e[t];
 }
 
 template <typename T>

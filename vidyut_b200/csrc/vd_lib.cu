@@ -141,7 +141,9 @@ void hier_build(Hier<T>& H, Alloc& A, const GridDev& fine, const double* dx, int
 {
     H.dim = fine.dim;
     H.varb = varb;
-    H.g.push_back(fine);
+    GridDev f0 = fine;
+    f0.rb = (fine.n[0] % 2 == 0) ? 1 : 0;
+    H.g.push_back(f0);
     H.dx.push_back({dx[0], dx[1], dx[2]});
     while ((int)H.g.size() - 1 < maxcoarsen)
     {
@@ -157,6 +159,7 @@ void hier_build(Hier<T>& H, Alloc& A, const GridDev& fine, const double* dx, int
             n.n[d] = c.n[d] / 2;
             ndx[d] = ndx[d] * 2.0;
         }
+        n.rb = (n.n[0] % 2 == 0) ? 1 : 0;
         H.g.push_back(n);
         H.dx.push_back(ndx);
     }
@@ -256,14 +259,47 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
 {
     const long long half = (long long)((op.g.n[0] + 1) / 2) * op.g.n[1] * op.g.n[2];
     const bool prof = t_prof && prof_tag != VD_PROF_NONE && t_prof->id == prof_tag;
-    if (prof) t_prof->bytes = double(2 * sizeof(T)) * (double)op.g.ncell();
+    // one colour: read the other colour of x and this colour of f, write
+    // this colour of x (plus the face coefficients when they vary)
+    if (prof)
+        t_prof->bytes = double(3 * sizeof(T)) / 2.0 * (double)op.g.ncell() +
+                        (op.b[0] ? double(op.g.dim * sizeof(T)) * (double)op.g.ncell() : 0.0);
     for (int s = 0; s < n; ++s)
         for (int color = 0; color < 2; ++color)
         {
             if (prof) t_prof->begin(st);
-            LAUNCH(k_mg_smooth_color<T>, gsz(half), BS, st, op, x, f, color, inh ? 1 : 0);
+            if (op.g.rb)
+            {
+                const int nxh = op.g.n[0] / 2;
+                const int bx = nxh >= 128 ? 128 : (nxh >= 64 ? 64 : 32);
+                const dim3 grid((nxh + bx - 1) / bx, op.g.n[1], op.g.n[2]);
+                if (op.b[0])
+                    LAUNCH((k_mg_smooth_rb<T, true>), grid, bx, st, op, x, f, color,
+                           inh ? 1 : 0, T(0));
+                else
+                {
+                    // interior diagonal of the constant-coefficient operator
+                    T gamma = op.aconst;
+                    for (int d = 0; d < op.g.dim; ++d) gamma += op.dh[d] * (op.bconst + op.bconst);
+                    LAUNCH((k_mg_smooth_rb<T, false>), grid, bx, st, op, x, f, color,
+                           inh ? 1 : 0, T(1) / gamma);
+                }
+            } else
+                LAUNCH(k_mg_smooth_color<T>, gsz(half), BS, st, op, x, f, color, inh ? 1 : 0);
             if (prof) t_prof->end(st);
         }
+}
+
+// Launch shape over the cells of a grid: x-blocks along rows, y = j, z = k.
+struct Grid3
+{
+    dim3 g, b;
+};
+Grid3 rows3(const GridDev& g, int ydiv = 1)
+{
+    const int nx = g.n[0];
+    const int bx = nx >= 128 ? 128 : (nx >= 64 ? 64 : 32);
+    return {dim3((nx + bx - 1) / bx, (g.n[1] + ydiv - 1) / ydiv, g.n[2]), dim3(bx)};
 }
 
 template <typename T>
@@ -282,10 +318,11 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
     const int L = H.nlev;
     if (L == 1)
     {
-        LAUNCH(k_mg_resid_norm<T>, gsz(H.g[0].ncell()), BS, st, H.op[0], x0, f0, H.t0f, dscr,
-               inh0 ? 1 : 0);
+        const Grid3 gn = rows3(H.g[0], 8);
+        LAUNCH(k_mg_resid_norm<T>, gn.g, gn.b, st, H.op[0], x0, f0, H.t0f, dscr, inh0 ? 1 : 0,
+               0, 8);
         bottom(H, H.op[0], H.t0x, H.t0f, st);
-        LAUNCH(k_mg_prolong_add<T>, gsz(H.g[0].ncell()), BS, st, H.g[0], H.g[0], x0, H.t0x);
+        LAUNCH(k_add_same<T>, gsz(H.g[0].ncell()), BS, st, x0, H.t0x, H.g[0].ncell());
         return;
     }
     for (int l = 0; l < L - 1; ++l)
@@ -294,8 +331,9 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         T* fl = l ? H.f[l] : f0;
         const bool inh = (l == 0) && inh0;
         smooth(H.op[l], xl, fl, inh, H.nu1, st, l == 0 ? H.prof_tag : VD_PROF_NONE);
-        LAUNCH(k_mg_resid_restrict<T>, gsz(H.g[l + 1].ncell()), BS, st, H.op[l], xl, fl,
-               H.g[l + 1], H.f[l + 1], H.x[l + 1], inh ? 1 : 0);
+        const Grid3 gr = rows3(H.g[l + 1]);
+        LAUNCH(k_mg_resid_restrict<T>, gr.g, gr.b, st, H.op[l], xl, fl, H.g[l + 1], H.f[l + 1],
+               H.x[l + 1], inh ? 1 : 0);
     }
     bottom(H, H.op[L - 1], H.x[L - 1], H.f[L - 1], st);
     for (int l = L - 2; l >= 0; --l)
@@ -303,8 +341,8 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         T* xl = l ? H.x[l] : x0;
         T* fl = l ? H.f[l] : f0;
         const bool inh = (l == 0) && inh0;
-        LAUNCH(k_mg_prolong_add<T>, gsz(H.g[l].ncell()), BS, st, H.g[l], H.g[l + 1], xl,
-               H.x[l + 1]);
+        const Grid3 gp = rows3(H.g[l]);
+        LAUNCH(k_mg_prolong_add<T>, gp.g, gp.b, st, H.g[l], H.g[l + 1], xl, H.x[l + 1]);
         smooth(H.op[l], xl, fl, inh, H.nu2, st, l == 0 ? H.prof_tag : VD_PROF_NONE);
     }
 }
@@ -424,8 +462,9 @@ double resid_norm(Ctx& c, const MGOp<T>& op, const T* x, const T* f, T* rout, bo
                   double* fnorm = nullptr)
 {
     VD_CUDA_OK(cudaMemsetAsync(c.dscal, 0, 2 * sizeof(unsigned long long), c.st));
-    LAUNCH(k_mg_resid_norm<T>, gsz(op.g.ncell()), BS, c.st, op, x, f, rout, c.dscal,
-           inh ? 1 : 0, fnorm ? 1 : 0);
+    const Grid3 gn = rows3(op.g, 8);
+    LAUNCH(k_mg_resid_norm<T>, gn.g, gn.b, c.st, op, x, f, rout, c.dscal, inh ? 1 : 0,
+           fnorm ? 1 : 0, 8);
     if (fnorm)
     {
         VD_CUDA_OK(cudaMemcpyAsync(c.hscal + 1, c.dscal + 1, sizeof(unsigned long long),
@@ -561,7 +600,7 @@ void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats)
 {
     const vd_config& cfg = c.cfg;
     const double ps = cfg.potential_scale;
-    LAUNCH(k_poisson_rhs, gsz(c.N), BS, c.st, c.G, Sold, c.S, c.phi_rhs, c.phi_sol,
+    LAUNCH(k_poisson_rhs, gsz(c.N), BS, c.st, c.G, c.HP.g[0], Sold, c.S, c.phi_rhs, c.phi_sol,
            cfg.do_spacechrg, cfg.poisson_warm_start, ps, time, c.dpp);
     fill_bc(c, 0, POT_ID, c.pbct, 2, 1.0 / ps, time, c.pside);
     hier_set_ops(c.HP, 0.0, 1.0, -1.0, c.pbct, 2);
@@ -574,7 +613,7 @@ void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats)
     }
     for (int s = 0; s < 6; ++s)
         if (c.pbct[s] == MG_INNEU)
-            LAUNCH(k_inneu_adjust, gsz(plane_count(c.g, s % 3)), BS, c.st, c.g, s,
+            LAUNCH(k_inneu_adjust, gsz(plane_count(c.g, s % 3)), BS, c.st, c.HP.g[0], s,
                    (const double*)nullptr, -1.0, 1.0, c.G.dx[s % 3], c.pside[s].val, c.phi_rhs);
     vd_solve_stats st{};
     const int it = mg_solve(c, c.HP, c.HP32, c.phi_sol, c.phi_rhs, &st);
@@ -655,8 +694,8 @@ void species_solve(Ctx& c, int comp, double time, const double* Sold, vd_solve_s
     for (int d = 0; d < cfg.dim; ++d)
         LAUNCH(k_species_faces, gsz(face_count(c.g, d)), BS, c.st, c.g, d, c.S, comp,
                cfg.gas_temperature, c.HS.bf[0][d]);
-    LAUNCH(k_species_rhs, gsz(c.N), BS, c.st, c.g, c.S, Sold, c.expl, comp, cfg.dt, ts, scale,
-           c.spec_rhs, c.u[comp]);
+    LAUNCH(k_species_rhs, gsz(c.N), BS, c.st, c.g, c.HS.g[0], c.S, Sold, c.expl, comp, cfg.dt,
+           ts, scale, c.spec_rhs, c.u[comp]);
     fill_bc(c, 1, comp, bct, 3, 1.0 / scale, time, c.sside);
     hier_set_ops(c.HS, (1.0 / cfg.dt) * ts * 1.0, ts, 1.0, bct, 3);
     hier_coarsen_coeffs(c.HS, bct, c.st);
@@ -674,7 +713,7 @@ void species_solve(Ctx& c, int comp, double time, const double* Sold, vd_solve_s
     }
     for (int s = 0; s < 6; ++s)
         if (bct[s] == MG_INNEU)
-            LAUNCH(k_inneu_adjust, gsz(plane_count(c.g, s % 3)), BS, c.st, c.g, s,
+            LAUNCH(k_inneu_adjust, gsz(plane_count(c.g, s % 3)), BS, c.st, c.HS.g[0], s,
                    (const double*)c.HS.bf[0][s % 3], 1.0, ts, c.G.dx[s % 3], c.sside[s].val,
                    c.spec_rhs);
     vd_solve_stats st{};
@@ -690,6 +729,7 @@ void joule(Ctx& c)
     P.phi_sol = c.phi_sol;
     P.ps = c.cfg.potential_scale;
     P.ue = c.u[c.eidx];
+    P.gm = c.HS.g[0];
     P.escale = c.cfg.species_scale[c.eidx];
     P.S = c.S;
     P.expl = c.expl;
@@ -716,6 +756,7 @@ FinalParams final_params(Ctx& c)
     P.rxn_een = c.rxn_een;
     P.expl = c.expl;
     P.dt = c.cfg.dt;
+    P.gm = c.HS.g[0];
     for (int sp = 0; sp < NUM_SPECIES; ++sp) P.bg[sp] = c.bg[sp];
     return P;
 }

@@ -80,35 +80,66 @@ __device__ __forceinline__ T mg_face_b(const MGOp<T>& L, int d, int i, int j, in
     return L.b[d][face_index(L.g, d, i, j, k)];
 }
 
-// Value of the neighbour of boundary-adjacent cell (i,j,k) one step along d
-// in direction sg; `cf` returns the coefficient of x0 inside a ghost value.
-template <typename T>
+// Value of the neighbour of cell (i,j,k) one step along D in direction sg,
+// through the boundary closure when it falls outside the level; `cf`
+// returns the coefficient of x0 inside a ghost value (0 for real cells).
+template <int D, typename T>
 __device__ __forceinline__ T mg_nbr(const MGOp<T>& L, const T* __restrict__ x, int i,
-                                    int j, int k, int d, int sg, bool inhomog, T x0,
-                                    T& cf)
+                                    int j, int k, int sg, bool inhomog, T x0, T& cf)
 {
-    int c[3] = {i, j, k};
-    c[d] += sg;
+    int ii = i, jj = j, kk = k;
+    int& c = (D == 0) ? ii : ((D == 1) ? jj : kk);
+    c += sg;
     cf = T(0);
-    if (c[d] >= 0 && c[d] < L.g.n[d]) return x[L.g.idx(c[0], c[1], c[2])];
-    if (L.g.per[d])
+    const int n = L.g.n[D];
+    if (c >= 0 && c < n) return x[L.g.idx(ii, jj, kk)];
+    if (L.g.per[D])
     {
-        c[d] = (c[d] + L.g.n[d]) % L.g.n[d];
-        return x[L.g.idx(c[0], c[1], c[2])];
+        c = (c + n) % n;
+        return x[L.g.idx(ii, jj, kk)];
     }
-    const int s = d + (sg > 0 ? 3 : 0);
-    const int p = plane_index(L.g, d, i, j, k);
+    const int s = D + (sg > 0 ? 3 : 0);
+    const int p = (D == 0) ? (j + L.g.n[1] * k) : ((D == 1) ? (i + L.g.n[0] * k) : (i + L.g.n[0] * j));
     const T c0 = L.c0[s] ? L.c0[s][p] : L.c0s[s];
     T gh = c0 * x0;
     if (L.c1s[s] != T(0))
     {
-        int m[3] = {i, j, k};
-        m[d] -= sg;
-        gh += L.c1s[s] * x[L.g.idx(m[0], m[1], m[2])];
+        int mi = i, mj = j, mk = k;
+        int& m = (D == 0) ? mi : ((D == 1) ? mj : mk);
+        m -= sg;
+        gh += L.c1s[s] * x[L.g.idx(mi, mj, mk)];
     }
     if (inhomog && L.gv[s]) gh += L.gv[s][p];
     cf = c0;
     return gh;
+}
+
+template <int D, typename T>
+__device__ __forceinline__ void mg_face_pair(const MGOp<T>& L, int i, int j, int k, T& blo,
+                                             T& bhi)
+{
+    if (!L.b[D])
+    {
+        blo = bhi = L.bconst;
+        return;
+    }
+    const long long f = face_index(L.g, D, i, j, k);
+    const long long st = (D == 0) ? 1
+                         : (D == 1) ? (long long)L.g.n[0]
+                                    : (long long)L.g.n[0] * L.g.n[1];
+    blo = L.b[D][f];
+    bhi = L.b[D][f + st];
+}
+
+template <int D, typename T>
+__device__ __forceinline__ void mg_term(const MGOp<T>& L, const T* __restrict__ x, int i,
+                                        int j, int k, bool inhomog, T x0, T& y)
+{
+    T blo, bhi, cf;
+    mg_face_pair<D>(L, i, j, k, blo, bhi);
+    const T xm = mg_nbr<D>(L, x, i, j, k, -1, inhomog, x0, cf);
+    const T xp = mg_nbr<D>(L, x, i, j, k, +1, inhomog, x0, cf);
+    y -= L.dh[D] * (bhi * (xp - x0) - blo * (x0 - xm));
 }
 
 template <typename T>
@@ -118,18 +149,24 @@ __device__ __forceinline__ T mg_apply(const MGOp<T>& L, const T* __restrict__ x,
     const long long p = L.g.idx(i, j, k);
     const T x0 = x[p];
     T y = (L.a ? L.a[p] : L.aconst) * x0;
-    for (int d = 0; d < L.g.dim; ++d)
-    {
-        int c[3] = {i, j, k};
-        const T blo = mg_face_b(L, d, c[0], c[1], c[2]);
-        c[d] += 1;
-        const T bhi = mg_face_b(L, d, c[0], c[1], c[2]);
-        T cf;
-        const T xm = mg_nbr(L, x, i, j, k, d, -1, inhomog, x0, cf);
-        const T xp = mg_nbr(L, x, i, j, k, d, +1, inhomog, x0, cf);
-        y -= L.dh[d] * (bhi * (xp - x0) - blo * (x0 - xm));
-    }
+    mg_term<0>(L, x, i, j, k, inhomog, x0, y);
+    if (L.g.dim > 1) mg_term<1>(L, x, i, j, k, inhomog, x0, y);
+    if (L.g.dim > 2) mg_term<2>(L, x, i, j, k, inhomog, x0, y);
     return y;
+}
+
+template <int D, typename T>
+__device__ __forceinline__ void mg_gs_term(const MGOp<T>& L, const T* __restrict__ x, int i,
+                                           int j, int k, bool inhomog, T x0, T& gamma,
+                                           T& rho, T& delta)
+{
+    T blo, bhi, cfm, cfp;
+    mg_face_pair<D>(L, i, j, k, blo, bhi);
+    gamma += L.dh[D] * (blo + bhi);
+    const T xm = mg_nbr<D>(L, x, i, j, k, -1, inhomog, x0, cfm);
+    const T xp = mg_nbr<D>(L, x, i, j, k, +1, inhomog, x0, cfp);
+    rho += L.dh[D] * (blo * xm + bhi * xp);
+    delta += L.dh[D] * (blo * cfm + bhi * cfp);
 }
 
 // Gauss-Seidel update of one cell in place.
@@ -142,21 +179,17 @@ __device__ __forceinline__ void mg_gs_cell(const MGOp<T>& L, T* __restrict__ x,
     const T x0 = x[p];
     T gamma = L.a ? L.a[p] : L.aconst;
     T rho = T(0), delta = T(0);
-    for (int d = 0; d < L.g.dim; ++d)
-    {
-        int c[3] = {i, j, k};
-        const T blo = mg_face_b(L, d, c[0], c[1], c[2]);
-        c[d] += 1;
-        const T bhi = mg_face_b(L, d, c[0], c[1], c[2]);
-        gamma += L.dh[d] * (blo + bhi);
-        T cfm, cfp;
-        const T xm = mg_nbr(L, x, i, j, k, d, -1, inhomog, x0, cfm);
-        const T xp = mg_nbr(L, x, i, j, k, d, +1, inhomog, x0, cfp);
-        rho += L.dh[d] * (blo * xm + bhi * xp);
-        delta += L.dh[d] * (blo * cfm + bhi * cfp);
-    }
+    mg_gs_term<0>(L, x, i, j, k, inhomog, x0, gamma, rho, delta);
+    if (L.g.dim > 1) mg_gs_term<1>(L, x, i, j, k, inhomog, x0, gamma, rho, delta);
+    if (L.g.dim > 2) mg_gs_term<2>(L, x, i, j, k, inhomog, x0, gamma, rho, delta);
     const T res = f[p] - (gamma * x0 - rho);
     x[p] = x0 + res / (gamma - delta);
+}
+
+__device__ __forceinline__ bool mg_interior(const GridDev& g, int i, int j, int k)
+{
+    return i > 0 && i < g.n[0] - 1 && (g.dim < 2 || (j > 0 && j < g.n[1] - 1)) &&
+           (g.dim < 3 || (k > 0 && k < g.n[2] - 1));
 }
 
 // ---------------------------------------------------------------- kernels
@@ -179,62 +212,184 @@ __global__ void k_mg_smooth_color(MGOp<T> L, T* __restrict__ x,
     }
 }
 
-// Residual f - L(x) at the 2^dim children of every coarse cell, averaged
-// into the coarse right-hand side; the coarse unknown is zeroed.
-template <typename T>
-__global__ void k_mg_resid_restrict(MGOp<T> L, const T* __restrict__ x,
-                                    const T* __restrict__ f, GridDev gc,
-                                    T* __restrict__ fc, T* __restrict__ xc, int inhomog)
+// One Gauss-Seidel colour on a red-black split level, launched on a grid
+// (half-row blocks, ny, nz): the thread's cell and its six neighbours are
+// unit-stride loads from the two colour halves.  Interior cells take the
+// branch-free path (constant coefficients use the precomputed 1/diagonal);
+// boundary cells the general one.
+template <typename T, bool VARB>
+__global__ void __launch_bounds__(128) k_mg_smooth_rb(MGOp<T> L, T* __restrict__ x,
+                                                      const T* __restrict__ f, int color,
+                                                      int inhomog, T inv_gamma)
 {
-    const long long tot = gc.ncell();
-    const int rz = (L.g.dim == 3) ? 2 : 1;
-    const T w = (L.g.dim == 3) ? T(0.125) : T(0.25);
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
-         t += (long long)gridDim.x * blockDim.x)
+    const GridDev& g = L.g;
+    const int nxh = g.n[0] >> 1;
+    const int ih = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ih >= nxh) return;
+    const int j = blockIdx.y, k = blockIdx.z;
+    const long long half = g.ncell() >> 1;
+    const long long plane = (long long)nxh * g.n[1];
+    const long long r = j + (long long)g.n[1] * k;
+    const long long h = ih + (long long)nxh * r;
+    const int q = (j + k + color) & 1;
+    const int i = 2 * ih + q;
+    if (!mg_interior(g, i, j, k))
     {
-        const int I = (int)(t % gc.n[0]);
-        const long long r = t / gc.n[0];
-        const int J = (int)(r % gc.n[1]);
-        const int K = (int)(r / gc.n[1]);
-        T s = T(0);
-        for (int kk = 0; kk < rz; ++kk)
-            for (int jj = 0; jj < 2; ++jj)
-                for (int ii = 0; ii < 2; ++ii)
-                {
-                    const int i = 2 * I + ii, j = 2 * J + jj, k = rz * K + kk;
-                    s += f[L.g.idx(i, j, k)] - mg_apply(L, x, i, j, k, inhomog != 0);
-                }
-        fc[t] = s * w;
-        if (xc) xc[t] = T(0);
+        mg_gs_cell(L, x, f, i, j, k, inhomog != 0);
+        return;
+    }
+    T* __restrict__ xs = x + color * half;
+    const T* __restrict__ xo = x + (1 - color) * half;
+    const T x0 = xs[h];
+    const T xm = xo[h - 1 + q], xp = xo[h + q];
+    const T ym = xo[h - nxh], yp = xo[h + nxh];
+    const T dhx = L.dh[0], dhy = L.dh[1], dhz = L.dh[2];
+    const T fv = f[color * half + h];
+    if (VARB)
+    {
+        const long long fx = i + (long long)(g.n[0] + 1) * r;
+        const T bxl = L.b[0][fx], bxh = L.b[0][fx + 1];
+        const long long fy = i + (long long)g.n[0] * (j + (long long)(g.n[1] + 1) * k);
+        const T byl = L.b[1][fy], byh = L.b[1][fy + g.n[0]];
+        T gamma = L.aconst;
+        gamma += dhx * (bxl + bxh);
+        gamma += dhy * (byl + byh);
+        T rho = dhx * (bxl * xm + bxh * xp);
+        rho += dhy * (byl * ym + byh * yp);
+        if (g.dim == 3)
+        {
+            const long long fz = i + (long long)g.n[0] * r;
+            const T bzl = L.b[2][fz], bzh = L.b[2][fz + (long long)g.n[0] * g.n[1]];
+            const T zm = xo[h - plane], zp = xo[h + plane];
+            gamma += dhz * (bzl + bzh);
+            rho += dhz * (bzl * zm + bzh * zp);
+        }
+        const T res = fv - (gamma * x0 - rho);
+        xs[h] = x0 + res / gamma;
+    } else
+    {
+        const T b = L.bconst;
+        T rho = dhx * (b * xm + b * xp);
+        rho += dhy * (b * ym + b * yp);
+        if (g.dim == 3) rho += dhz * (b * xo[h - plane] + b * xo[h + plane]);
+        // x0 + (f - (gamma x0 - rho)) / gamma = (f + rho) / gamma
+        xs[h] = (fv + rho) * inv_gamma;
     }
 }
 
-// Max-norm of f - L(x) into mx[0] (and of f into mx[1] when `fnorm`).
+// L(x) at an interior cell of a red-black split level, neighbours addressed
+// directly in the two colour halves (same arithmetic as mg_apply).
 template <typename T>
-__global__ void k_mg_resid_norm(MGOp<T> L, const T* __restrict__ x,
-                                const T* __restrict__ f, T* __restrict__ rout,
-                                unsigned long long* mx, int inhomog, int fnorm = 0)
+__device__ __forceinline__ T mg_apply_rb(const MGOp<T>& L, const T* __restrict__ x, int i,
+                                         int j, int k)
+{
+    const GridDev& g = L.g;
+    const int nxh = g.n[0] >> 1;
+    const long long half = g.ncell() >> 1;
+    const int color = (i + j + k) & 1, q = i & 1;
+    const long long r = j + (long long)g.n[1] * k;
+    const long long h = (i >> 1) + (long long)nxh * r;
+    const T* __restrict__ xs = x + color * half;
+    const T* __restrict__ xo = x + (1 - color) * half;
+    const T x0 = xs[h];
+    const T xm = xo[h - 1 + q], xp = xo[h + q];
+    const T ym = xo[h - nxh], yp = xo[h + nxh];
+    T bxl, bxh, byl, byh;
+    if (L.b[0])
+    {
+        const long long fx = i + (long long)(g.n[0] + 1) * r;
+        bxl = L.b[0][fx];
+        bxh = L.b[0][fx + 1];
+        const long long fy = i + (long long)g.n[0] * (j + (long long)(g.n[1] + 1) * k);
+        byl = L.b[1][fy];
+        byh = L.b[1][fy + g.n[0]];
+    } else
+        bxl = bxh = byl = byh = L.bconst;
+    T y = L.aconst * x0;
+    y -= L.dh[0] * (bxh * (xp - x0) - bxl * (x0 - xm));
+    y -= L.dh[1] * (byh * (yp - x0) - byl * (x0 - ym));
+    if (g.dim == 3)
+    {
+        const long long plane = (long long)nxh * g.n[1];
+        const T zm = xo[h - plane], zp = xo[h + plane];
+        T bzl, bzh;
+        if (L.b[2])
+        {
+            const long long fz = i + (long long)g.n[0] * r;
+            bzl = L.b[2][fz];
+            bzh = L.b[2][fz + (long long)g.n[0] * g.n[1]];
+        } else
+            bzl = bzh = L.bconst;
+        y -= L.dh[2] * (bzh * (zp - x0) - bzl * (x0 - zm));
+    }
+    return y;
+}
+
+template <typename T>
+__device__ __forceinline__ T mg_apply_any(const MGOp<T>& L, const T* __restrict__ x, int i,
+                                          int j, int k, bool inhomog)
+{
+    if (L.g.rb && !L.a && mg_interior(L.g, i, j, k)) return mg_apply_rb(L, x, i, j, k);
+    return mg_apply(L, x, i, j, k, inhomog);
+}
+
+// Residual f - L(x) at the 2^dim children of every coarse cell, averaged
+// into the coarse right-hand side; the coarse unknown is zeroed.  Grid:
+// (coarse-row blocks, coarse ny, coarse nz).
+template <typename T>
+__global__ void __launch_bounds__(128) k_mg_resid_restrict(MGOp<T> L, const T* __restrict__ x,
+                                                           const T* __restrict__ f, GridDev gc,
+                                                           T* __restrict__ fc,
+                                                           T* __restrict__ xc, int inhomog)
+{
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= gc.n[0]) return;
+    const int J = blockIdx.y, K = blockIdx.z;
+    const int rz = (L.g.dim == 3) ? 2 : 1;
+    const T w = (L.g.dim == 3) ? T(0.125) : T(0.25);
+    T s = T(0);
+    for (int kk = 0; kk < rz; ++kk)
+        for (int jj = 0; jj < 2; ++jj)
+            for (int ii = 0; ii < 2; ++ii)
+            {
+                const int i = 2 * I + ii, j = 2 * J + jj, k = rz * K + kk;
+                s += f[L.g.idx(i, j, k)] - mg_apply_any(L, x, i, j, k, inhomog != 0);
+            }
+    const long long pc = gc.idx(I, J, K);
+    fc[pc] = s * w;
+    if (xc) xc[pc] = T(0);
+}
+
+// Max-norm of f - L(x) into mx[0] (and of f into mx[1] when `fnorm`); the
+// residual itself into rout when given.  Grid: (row blocks, ny/rows, nz),
+// each thread walking `rows` rows.
+template <typename T>
+__global__ void __launch_bounds__(128) k_mg_resid_norm(MGOp<T> L, const T* __restrict__ x,
+                                                       const T* __restrict__ f,
+                                                       T* __restrict__ rout,
+                                                       unsigned long long* mx, int inhomog,
+                                                       int fnorm, int rows)
 {
     __shared__ double sh[32];
-    const long long tot = L.g.ncell();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.z;
     double m = 0.0, mf = 0.0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
-         t += (long long)gridDim.x * blockDim.x)
-    {
-        const int i = (int)(t % L.g.n[0]);
-        const long long r = t / L.g.n[0];
-        const int j = (int)(r % L.g.n[1]);
-        const int k = (int)(r / L.g.n[1]);
-        const T rr = f[t] - mg_apply(L, x, i, j, k, inhomog != 0);
-        if (rout) rout[t] = rr;
-        const double a = fabs((double)rr);
-        m = a > m ? a : m;
-        if (fnorm)
+    if (i < L.g.n[0])
+        for (int jj = 0; jj < rows; ++jj)
         {
-            const double af = fabs((double)f[t]);
-            mf = af > mf ? af : mf;
+            const int j = blockIdx.y * rows + jj;
+            if (j >= L.g.n[1]) break;
+            const long long p = L.g.idx(i, j, k);
+            const T rr = f[p] - mg_apply_any(L, x, i, j, k, inhomog != 0);
+            if (rout) rout[p] = rr;
+            const double a = fabs((double)rr);
+            m = a > m ? a : m;
+            if (fnorm)
+            {
+                const double af = fabs((double)f[p]);
+                mf = af > mf ? af : mf;
+            }
         }
-    }
     m = block_max(m, sh);
     if (threadIdx.x == 0) atomic_max_nonneg(mx, m);
     if (fnorm)
@@ -245,25 +400,21 @@ __global__ void k_mg_resid_norm(MGOp<T> L, const T* __restrict__ x,
 }
 
 template <typename T>
-__global__ void k_mg_prolong_add(GridDev gf, GridDev gc, T* __restrict__ xf,
-                                 const T* __restrict__ xc)
+__global__ void __launch_bounds__(128) k_mg_prolong_add(GridDev gf, GridDev gc,
+                                                        T* __restrict__ xf,
+                                                        const T* __restrict__ xc)
 {
-    const long long tot = gf.ncell();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= gf.n[0]) return;
+    const int j = blockIdx.y, k = blockIdx.z;
     const int rz = (gf.dim == 3) ? 2 : 1;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
-         t += (long long)gridDim.x * blockDim.x)
-    {
-        const int i = (int)(t % gf.n[0]);
-        const long long r = t / gf.n[0];
-        const int j = (int)(r % gf.n[1]);
-        const int k = (int)(r / gf.n[1]);
-        xf[t] += xc[gc.idx(i >> 1, j >> 1, k / rz)];
-    }
+    xf[gf.idx(i, j, k)] += xc[gc.idx(i >> 1, j >> 1, k / rz)];
 }
 
 // BiCGStab on the coarsest level in one CTA (homogeneous boundaries),
 // relative tolerance `rel` on the max-norm, `maxiter` iterations, then `nub`
-// Gauss-Seidel smooths (or `nuf` when BiCGStab did not converge).
+// Gauss-Seidel smooths (or `nuf` when BiCGStab did not converge).  Every
+// vector is addressed through the level's layout (L.g.idx), like x and b.
 template <typename T>
 __global__ void k_mg_bottom(MGOp<T> L, T* __restrict__ x, const T* __restrict__ b,
                             T* __restrict__ scr, T rel, int maxiter, int nub, int nuf,
@@ -278,12 +429,7 @@ __global__ void k_mg_bottom(MGOp<T> L, T* __restrict__ x, const T* __restrict__ 
     T* s = scr + 4 * n;
     T* tt = scr + 5 * n;
     const int tid = threadIdx.x, bs = blockDim.x;
-    auto cell = [&](long long q, int& i, int& j, int& k) {
-        i = (int)(q % L.g.n[0]);
-        const long long rr = q / L.g.n[0];
-        j = (int)(rr % L.g.n[1]);
-        k = (int)(rr / L.g.n[1]);
-    };
+    const int nx = L.g.n[0], ny = L.g.n[1];
     T m = T(0);
     for (long long q = tid; q < n; q += bs)
     {
@@ -322,10 +468,10 @@ __global__ void k_mg_bottom(MGOp<T> L, T* __restrict__ x, const T* __restrict__ 
             }
             __syncthreads();
             acc = T(0);
-            for (long long q = tid; q < n; q += bs)
+            for (long long c = tid; c < n; c += bs)
             {
-                int i, j, k;
-                cell(q, i, j, k);
+                const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+                const long long q = L.g.idx(i, j, k);
                 v[q] = mg_apply(L, p, i, j, k, false);
                 acc += rh[q] * v[q];
             }
@@ -350,10 +496,10 @@ __global__ void k_mg_bottom(MGOp<T> L, T* __restrict__ x, const T* __restrict__ 
                 break;
             }
             T a1 = T(0), a2 = T(0);
-            for (long long q = tid; q < n; q += bs)
+            for (long long c = tid; c < n; c += bs)
             {
-                int i, j, k;
-                cell(q, i, j, k);
+                const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+                const long long q = L.g.idx(i, j, k);
                 tt[q] = mg_apply(L, s, i, j, k, false);
                 a1 += tt[q] * tt[q];
                 a2 += tt[q] * s[q];
@@ -392,10 +538,9 @@ __global__ void k_mg_bottom(MGOp<T> L, T* __restrict__ x, const T* __restrict__ 
     for (int sm = 0; sm < nsm; ++sm)
         for (int color = 0; color < 2; ++color)
         {
-            for (long long q = tid; q < n; q += bs)
+            for (long long c = tid; c < n; c += bs)
             {
-                int i, j, k;
-                cell(q, i, j, k);
+                const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
                 if (((i + j + k + color) & 1) == 0) mg_gs_cell(L, x, b, i, j, k, false);
             }
             __syncthreads();
