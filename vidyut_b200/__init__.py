@@ -121,10 +121,8 @@ def load(case: str) -> C.CDLL:
     """Load (building on first use if absent) the CUDA library of `case`."""
     if case in _LIBS:
         return _LIBS[case]
-    path = lib_path(case)
-    if not os.path.exists(path):
-        from . import build
-        build.build_case(case)
+    from . import build
+    path = build.build_case(case)  # no-op unless missing or older than its sources
     lib = C.CDLL(path)
     P = C.c_void_p
     sig = {
