@@ -240,6 +240,34 @@ vd_status vd_profile_read(void* ctx, long long* launches, double* total_ms,
  * vd_create when ctx is NULL). */
 vd_status vd_last_error(void* ctx, char* buf, int len);
 
+/* Poisson solve that allocates no device memory.  No counterpart in the
+ * reference: it serves callers that must not allocate device memory while
+ * they run, e.g. a host framework whose own memory pool owns the whole
+ * device, or code that cannot afford an allocation's implicit device
+ * synchronisation.  It solves del^2 phi = rhs (the field solve's operator,
+ * second-order Dirichlet closure) with the same red-black multigrid as
+ * vd_poisson_solve and the same convergence test, on the current device.
+ *   rhs, phi   caller-owned device arrays of n_cell[0]*n_cell[1]*n_cell[2]
+ *              doubles, x fastest; phi holds the initial guess on entry and
+ *              the solution on return;
+ *   bc_lo/hi   PERBC, DIRCBC or HNEUBC per direction; bcval_lo/hi the
+ *              Dirichlet face values (may be NULL for all zero);
+ *   err        optional buffer for a message (NULL to skip).
+ * Its multigrid scratch is one fixed array of 8 MiB per device, built into
+ * the library and held by every device that loads it until the process
+ * exits; grids needing more (above about 128^3 cells) are rejected with
+ * VD_ERR_INVALID_ARG and a message saying how much they need.  The first
+ * call on a device looks up that array's device address (with the device
+ * current), so make that first call before any stream capture.  Work runs on
+ * the legacy default stream; every call reuses the same scratch, so calls
+ * that overlap on one device race and must be serialised by the caller. */
+vd_status vd_poisson_solve_noalloc(int dim, const int* n_cell, const double* dx,
+                                   const int* bc_lo, const int* bc_hi,
+                                   const double* bcval_lo, const double* bcval_hi,
+                                   const double* rhs, double* phi, double reltol,
+                                   double abstol, int maxiter, vd_solve_stats* stats,
+                                   char* err, int errlen);
+
 #ifdef __cplusplus
 }
 #endif

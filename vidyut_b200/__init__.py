@@ -95,7 +95,7 @@ EXPORTS = [
     "vd_init_domain", "vd_set_state", "vd_get_state", "vd_set_time", "vd_get_time",
     "vd_step", "vd_poisson_solve", "vd_explicit_rhs", "vd_implicit_diffusion",
     "vd_check_state", "vd_launch_count", "vd_profile_kernel", "vd_profile_read",
-    "vd_last_error",
+    "vd_last_error", "vd_poisson_solve_noalloc",
 ]
 
 VD_PROF_NONE = 0
@@ -146,6 +146,11 @@ def load(case: str) -> C.CDLL:
         "vd_profile_read": [P, C.POINTER(C.c_longlong), C.POINTER(C.c_double),
                             C.POINTER(C.c_double)],
         "vd_last_error": [P, C.c_char_p, C.c_int],
+        "vd_poisson_solve_noalloc": [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_double), P, P,
+                                     C.c_double, C.c_double, C.c_int,
+                                     C.POINTER(vd_solve_stats), C.c_char_p, C.c_int],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

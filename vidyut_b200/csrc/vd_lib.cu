@@ -1363,3 +1363,319 @@ vd_status vd_last_error(void* ctx, char* buf, int len)
 }
 
 } // extern "C"
+
+// ======================================================================
+// Allocation-free Poisson solve.
+//
+// Some callers cannot call cudaMalloc at solve time: a host framework that
+// owns all device memory through its own pool and forbids allocation
+// inside its step (allocation would break its memory accounting), or code
+// running where a device allocation could synchronise the device or fail
+// late.  vd_poisson_solve_noalloc serves them: the caller passes the
+// right-hand side and the potential as device arrays it already owns, and
+// every scratch array the multigrid needs (coarse levels, boundary planes,
+// bottom-solver vectors, residual norms) lives in the file-scope device
+// array below, which every GPU that loads this library holds until the
+// process exits.
+// ======================================================================
+namespace {
+
+constexpr long long VD_NA_SCRATCH_DOUBLES = 1LL << 20; // 8 MiB per device
+constexpr int VD_NA_MAX_LEVELS = 16;
+constexpr int VD_NA_MAX_DEVICES = 64;
+
+static __device__ __align__(256) double vd_na_scratch[VD_NA_SCRATCH_DOUBLES];
+
+// Device address of vd_na_scratch per device, looked up once per device
+// with that device current (the host-side symbol is not a device address).
+double* g_na_ptr[VD_NA_MAX_DEVICES] = {};
+
+void na_msg(char* err, int errlen, const char* m)
+{
+    if (err && errlen > 0)
+    {
+        std::strncpy(err, m, errlen - 1);
+        err[errlen - 1] = 0;
+    }
+}
+
+#define NA_LAUNCH(K, G, B, ...)                                                   \
+    do                                                                            \
+    {                                                                             \
+        K<<<(G), (B), 0, 0>>>(__VA_ARGS__);                                       \
+        ++vd::g_launches;                                                         \
+        const cudaError_t e_ = cudaGetLastError();                                \
+        if (e_ != cudaSuccess)                                                    \
+        {                                                                         \
+            na_msg(err, errlen, cudaGetErrorString(e_));                          \
+            return VD_ERR_CUDA;                                                   \
+        }                                                                         \
+    } while (0)
+
+long long na_round(long long n) { return (n + 31) & ~31LL; }
+
+struct NAHier
+{
+    int nlev;
+    GridDev g[VD_NA_MAX_LEVELS];
+    double dx[VD_NA_MAX_LEVELS][3];
+    double* x[VD_NA_MAX_LEVELS];
+    double* f[VD_NA_MAX_LEVELS];
+    MGOp<double> op[VD_NA_MAX_LEVELS];
+    double* g0[6];
+    double* scratch;
+    double* t0x;
+    double* t0f;
+    unsigned long long* norm;
+};
+
+int na_vcycle(NAHier& H, double* x0, const double* f0, char* err, int errlen)
+{
+    const int L = H.nlev;
+    if (L == 1)
+    {
+        const Grid3 gn = rows3(H.g[0], 8);
+        NA_LAUNCH(k_mg_resid_norm<double>, gn.g, gn.b, H.op[0], x0, f0, H.t0f, H.norm + 2, 1,
+                  0, 8);
+        NA_LAUNCH(k_mg_bottom<double>, 1, 256, H.op[0], H.t0x, H.t0f, H.scratch, 1e-4, 200, 0,
+                  8, (int*)nullptr);
+        NA_LAUNCH(k_add_same<double>, gsz(H.g[0].ncell()), BS, x0, H.t0x, H.g[0].ncell());
+        return VD_OK;
+    }
+    for (int l = 0; l < L; ++l)
+    {
+        double* xl = l ? H.x[l] : x0;
+        const double* fl = l ? H.f[l] : f0;
+        if (l == L - 1)
+        {
+            NA_LAUNCH(k_mg_bottom<double>, 1, 256, H.op[l], xl, fl, H.scratch, 1e-4, 200, 0, 8,
+                      (int*)nullptr);
+            break;
+        }
+        for (int s = 0; s < 2; ++s)
+            for (int color = 0; color < 2; ++color)
+                NA_LAUNCH(k_mg_smooth_color<double>,
+                          gsz((long long)((H.g[l].n[0] + 1) / 2) * H.g[l].n[1] * H.g[l].n[2]), BS,
+                          H.op[l], xl, fl, color, l == 0 ? 1 : 0);
+        const Grid3 gr = rows3(H.g[l + 1]);
+        NA_LAUNCH(k_mg_resid_restrict<double>, gr.g, gr.b, H.op[l], xl, fl, H.g[l + 1],
+                  H.f[l + 1], H.x[l + 1], l == 0 ? 1 : 0);
+    }
+    for (int l = L - 2; l >= 0; --l)
+    {
+        double* xl = l ? H.x[l] : x0;
+        const double* fl = l ? H.f[l] : f0;
+        const Grid3 gp = rows3(H.g[l]);
+        NA_LAUNCH(k_mg_prolong_add<double>, gp.g, gp.b, H.g[l], H.g[l + 1], xl, H.x[l + 1]);
+        for (int s = 0; s < 2; ++s)
+            for (int color = 0; color < 2; ++color)
+                NA_LAUNCH(k_mg_smooth_color<double>,
+                          gsz((long long)((H.g[l].n[0] + 1) / 2) * H.g[l].n[1] * H.g[l].n[2]), BS,
+                          H.op[l], xl, fl, color, l == 0 ? 1 : 0);
+    }
+    return VD_OK;
+}
+
+__global__ void k_na_fill_side(double* g, int np, double v)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x)
+        g[q] = v;
+}
+
+} // namespace
+
+extern "C" vd_status vd_poisson_solve_noalloc(int dim, const int* n_cell, const double* dx,
+                                              const int* bc_lo, const int* bc_hi,
+                                              const double* bcval_lo, const double* bcval_hi,
+                                              const double* rhs, double* phi, double reltol,
+                                              double abstol, int maxiter,
+                                              vd_solve_stats* stats, char* err, int errlen)
+{
+    if ((dim != 2 && dim != 3) || !n_cell || !dx || !bc_lo || !bc_hi || !rhs || !phi)
+    {
+        na_msg(err, errlen, "vd_poisson_solve_noalloc: bad arguments");
+        return VD_ERR_INVALID_ARG;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= VD_NA_MAX_DEVICES)
+    {
+        na_msg(err, errlen, "vd_poisson_solve_noalloc: no usable current CUDA device");
+        return VD_ERR_CUDA;
+    }
+    if (!g_na_ptr[dev])
+    {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, vd_na_scratch);
+        if (e != cudaSuccess || !p)
+        {
+            na_msg(err, errlen, cudaGetErrorString(e));
+            return VD_ERR_CUDA;
+        }
+        g_na_ptr[dev] = static_cast<double*>(p);
+    }
+    double* base = g_na_ptr[dev];
+
+    // level hierarchy (fine level: the caller's arrays, natural layout)
+    NAHier H{};
+    GridDev fine{};
+    fine.dim = dim;
+    for (int d = 0; d < 3; ++d)
+    {
+        fine.n[d] = d < dim ? n_cell[d] : 1;
+        fine.per[d] = (d < dim && bc_lo[d] == PERBC) ? 1 : 0;
+        if (fine.n[d] < 1 || (d < dim && !(dx[d] > 0.0)))
+        {
+            na_msg(err, errlen, "vd_poisson_solve_noalloc: bad grid");
+            return VD_ERR_INVALID_ARG;
+        }
+    }
+    fine.rb = 0;
+    H.g[0] = fine;
+    for (int d = 0; d < 3; ++d) H.dx[0][d] = d < dim ? dx[d] : 1.0;
+    H.nlev = 1;
+    while (H.nlev < VD_NA_MAX_LEVELS)
+    {
+        const GridDev& c = H.g[H.nlev - 1];
+        bool ok = true;
+        for (int d = 0; d < dim; ++d)
+            if (c.n[d] % 2 != 0 || c.n[d] / 2 < 2) ok = false;
+        if (!ok) break;
+        GridDev nxt = c;
+        for (int d = 0; d < dim; ++d)
+        {
+            nxt.n[d] = c.n[d] / 2;
+            H.dx[H.nlev][d] = H.dx[H.nlev - 1][d] * 2.0;
+        }
+        for (int d = dim; d < 3; ++d) H.dx[H.nlev][d] = 1.0;
+        nxt.rb = (nxt.n[0] % 2 == 0) ? 1 : 0;
+        H.g[H.nlev++] = nxt;
+    }
+    if (H.g[H.nlev - 1].ncell() > 4096)
+    {
+        na_msg(err, errlen, "vd_poisson_solve_noalloc: grid does not coarsen to 4096 cells");
+        return VD_ERR_INVALID_ARG;
+    }
+    // carve the scratch: norms, boundary planes, coarse levels, bottom vectors
+    long long off = 32;
+    for (int s = 0; s < 6; ++s)
+    {
+        H.g0[s] = base + off;
+        off += na_round(plane_count(fine, s % 3));
+    }
+    for (int l = 1; l < H.nlev; ++l)
+    {
+        H.x[l] = base + off;
+        off += na_round(H.g[l].ncell());
+        H.f[l] = base + off;
+        off += na_round(H.g[l].ncell());
+    }
+    H.scratch = base + off;
+    off += na_round(6 * H.g[H.nlev - 1].ncell());
+    if (H.nlev == 1)
+    {
+        H.t0x = base + off;
+        off += na_round(fine.ncell());
+        H.t0f = base + off;
+        off += na_round(fine.ncell());
+    }
+    if (off > VD_NA_SCRATCH_DOUBLES)
+    {
+        char m[256];
+        std::snprintf(m, sizeof(m),
+                      "vd_poisson_solve_noalloc: this grid needs %lld doubles of scratch, the "
+                      "allocation-free solve holds at most %lld (about 128^3 cells)",
+                      off, VD_NA_SCRATCH_DOUBLES);
+        na_msg(err, errlen, m);
+        return VD_ERR_INVALID_ARG;
+    }
+    H.norm = reinterpret_cast<unsigned long long*>(base);
+
+    // operator: del^2 phi = rhs  (a = 0, b = -1, beta = 1, maxorder 2),
+    // the field solve's operator (Source/PotentialSolve.cpp:205-219)
+    int bct[6];
+    for (int d = 0; d < 3; ++d)
+    {
+        if (d >= dim || fine.per[d])
+        {
+            bct[d] = bct[d + 3] = MG_PER;
+            continue;
+        }
+        bct[d] = mg_type(bc_lo[d]);
+        bct[d + 3] = mg_type(bc_hi[d]);
+        if ((bct[d] != MG_DIR && bct[d] != MG_NEU) || (bct[d + 3] != MG_DIR && bct[d + 3] != MG_NEU))
+        {
+            na_msg(err, errlen, "vd_poisson_solve_noalloc: boundaries must be periodic, "
+                                "Dirichlet or homogeneous Neumann");
+            return VD_ERR_UNSUPPORTED;
+        }
+    }
+    for (int l = 0; l < H.nlev; ++l)
+    {
+        MGOp<double>& o = H.op[l];
+        o = MGOp<double>{};
+        o.g = H.g[l];
+        for (int d = 0; d < 3; ++d) o.dh[d] = d < dim ? 1.0 / (H.dx[l][d] * H.dx[l][d]) : 0.0;
+        o.aconst = 0.0;
+        o.bconst = -1.0;
+        for (int s = 0; s < 6; ++s)
+        {
+            o.bct[s] = bct[s];
+            o.c0s[s] = 1.0;
+            o.c1s[s] = 0.0;
+            if (bct[s] == MG_DIR)
+            {
+                o.c0s[s] = -1.0;
+                if (l == 0) o.gv[s] = H.g0[s];
+            }
+        }
+    }
+    for (int s = 0; s < 6; ++s)
+        if (bct[s] == MG_DIR)
+        {
+            const int np = plane_count(fine, s % 3);
+            const double v = (s < 3 ? (bcval_lo ? bcval_lo[s] : 0.0) : (bcval_hi ? bcval_hi[s - 3] : 0.0));
+            NA_LAUNCH(k_na_fill_side, gsz(np), BS, H.g0[s], np, 2.0 * v);
+        }
+
+    // solve (max-norm test against max(|rhs|, |r0|), as the context path)
+    auto norm = [&](double* r, double* fmax) -> int {
+        if (cudaMemsetAsync(H.norm, 0, 2 * sizeof(unsigned long long), 0) != cudaSuccess)
+            return VD_ERR_CUDA;
+        const Grid3 gn = rows3(fine, 8);
+        NA_LAUNCH(k_mg_resid_norm<double>, gn.g, gn.b, H.op[0], phi, rhs, (double*)nullptr,
+                  H.norm, 1, fmax ? 1 : 0, 8);
+        unsigned long long h[2] = {0, 0};
+        if (cudaMemcpy(h, H.norm, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return VD_ERR_CUDA;
+        std::memcpy(r, &h[0], sizeof(double));
+        if (fmax) std::memcpy(fmax, &h[1], sizeof(double));
+        return VD_OK;
+    };
+    vd_solve_stats st{};
+    double r0 = 0.0, b0 = 0.0;
+    if (norm(&r0, &b0) != VD_OK)
+    {
+        na_msg(err, errlen, "vd_poisson_solve_noalloc: CUDA error");
+        return VD_ERR_CUDA;
+    }
+    const double target = std::max(abstol, std::max(reltol, 1e-16) * std::max(b0, r0));
+    st.initial_residual = st.final_residual = r0;
+    st.converged = (r0 <= target) ? 1 : 0;
+    for (int it = 1; !st.converged && it <= maxiter; ++it)
+    {
+        const int rc = na_vcycle(H, phi, rhs, err, errlen);
+        if (rc != VD_OK) return (vd_status)rc;
+        double rn = 0.0;
+        if (norm(&rn, nullptr) != VD_OK)
+        {
+            na_msg(err, errlen, "vd_poisson_solve_noalloc: CUDA error");
+            return VD_ERR_CUDA;
+        }
+        st.iterations = it;
+        st.final_residual = rn;
+        if (rn <= target) st.converged = 1;
+    }
+    if (stats) *stats = st;
+    na_msg(err, errlen, "");
+    return st.converged ? VD_OK : VD_ERR_NOT_CONVERGED;
+}
