@@ -12,7 +12,7 @@ One process per GPU (torchrun for N > 1); the path does not shard, so N > 1
 runs N independent replicas ("weak" scaling; barrier and max-over-ranks
 device time).  `--impl reference` times the CPU restatement of the reference
 step (the reference, an AMReX application, cannot be built here) on the host
-cores, rank 0 only, on a 128^3 sample of the same workload per step.
+cores, rank 0 only, on a 96^3 sample of the same workload per step.
 
 Timing: device time of the K steps from CUDA events on the library's stream;
 inputs (3.4 GB of state) exceed the 126 MB L2 between steps.
@@ -97,7 +97,9 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup():
+def dist_setup(backend: str | None = None):
+    """One process per GPU; the replicas exchange nothing but a barrier and
+    the max-over-ranks time (NCCL on GPUs, gloo for the CPU tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -107,9 +109,13 @@ def dist_setup():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        backend = backend or os.environ.get("VD_DIST_BACKEND", "nccl")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return world, rank, local, dist
 
 
@@ -117,9 +123,15 @@ def dist_max(dist, v: float) -> float:
     if dist is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(world: int, ncell: int, steps: int, max_ms: float) -> float:
+    """Whole-job cell-steps/s of `world` replicas timed by the slowest."""
+    return world * ncell * steps / (max_ms / 1e3)
 
 
 def barrier(dist):
@@ -155,7 +167,7 @@ def cpu_sample(steps: int, n: int = 128) -> dict:
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    n = 128
+    n = 96
     from oracle.oracle import Oracle
     from vidyut_b200 import workloads as W
     cfg = W.townsend_config(3, n)
@@ -199,6 +211,40 @@ def timed(g, steps: int, dist, prof_id: int):
     return st, l1 - l0, prof
 
 
+def adjoint_leg(device: int, dist, n: int = 128, nsteps: int = 50, K: int = 10) -> dict:
+    """Gradient of the electron count after 50 explicit LMEA steps at 128^3
+    (30 log pre-factors + electron mobility scale), checkpoints every 10:
+    device time of one forward-only pass and of one checkpointed adjoint run
+    (forward, recompute, backward), host synchronised on both sides."""
+    import torch
+    import vidyut_b200 as vb
+    from vidyut_b200 import workloads as W
+
+    cfg = W.adjoint_config(n, device=device)
+    g = vb.Vidyut(cfg)
+    g.set_state(0, W.adjoint_state(cfg, 0))
+    g.adjoint_run(5, K=5)  # warm-up
+    torch.cuda.synchronize()
+    barrier(dist)
+    t0 = time.perf_counter()
+    g.adjoint_forward(nsteps)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    J, grad = g.adjoint_run(nsteps, K=K)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    g.close()
+    fwd = dist_max(dist, t1 - t0)
+    run = dist_max(dist, t2 - t1)
+    return {"workload": f"LMEA 8 species / 30 reactions, {n}^3, {nsteps} explicit flux+source "
+                        f"steps at dt 1e-12 s, checkpoints every {K}, objective sum n_e dV, "
+                        "31 parameters",
+            "forward_ms": 1e3 * fwd, "adjoint_run_ms": 1e3 * run,
+            "adjoint_over_forward": run / fwd,
+            "forward_cell_steps_per_s": n ** 3 * nsteps / fwd,
+            "objective": J, "grad_norm": float(np.linalg.norm(grad))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -207,6 +253,9 @@ def main():
     ap.add_argument("--impl", default="vidyut_b200")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--lean", action="store_true",
+                    help="timed FP64 leg only (no e2e, FP32 or CPU legs): profiling runs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, dist = dist_setup()
@@ -233,7 +282,7 @@ def main():
     st, launches, prof = timed(g, args.steps, dist, vb.VD_PROF_POISSON_SMOOTH)
     clk = clocks.stop()
     ms = dist_max(dist, st.gpu_ms)
-    value = world * ncell * args.steps / (ms / 1e3)
+    value = replica_value(world, ncell, args.steps, ms)
 
     # roofline of the dominant kernel (fine-level Poisson RB sweep)
     peak, peak_kind = load_peaks()
@@ -247,6 +296,16 @@ def main():
             "algorithmic_bytes_per_launch": pbytes, "launches_timed": nl,
             "avg_launch_us": avg_s * 1e6 if nl else None,
             "traffic": (traffic or {}).get("bytes_per_launch") if traffic else None}
+
+    if args.lean:
+        if rank == 0:
+            print(json.dumps({"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s",
+                              "n_gpus": world, "steps": args.steps, "ms_per_step": ms / args.steps,
+                              "lean": True, "grid": [n, n, n], "roofline": roof}), flush=True)
+        g.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     # end to end through the C ABI with pinned host buffers: state in,
     # K steps, species + potential out, all inside the timed region
@@ -281,7 +340,7 @@ def main():
     g32.step(args.warmup)
     st32, _, _ = timed(g32, args.steps, dist, 0)
     ms32 = dist_max(dist, st32.gpu_ms)
-    value32 = world * ncell * args.steps / (ms32 / 1e3)
+    value32 = replica_value(world, ncell, args.steps, ms32)
     # Poisson error of the refined form against the FP64 form, same state
     ga, gb = vb.Vidyut(make(n, vb.VD_MG_FP64, local)), g32
     ga.set_state(0, state)
@@ -294,10 +353,12 @@ def main():
     ga.close()
     gb.close()
 
+    adj = None if args.no_adjoint else adjoint_leg(local, dist)
+
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
-            cpu = cpu_sample(1, 128)
+            cpu = cpu_sample(8, 128)
         line = {
             "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -319,6 +380,7 @@ def main():
                              "speedup_vs_fp64": value32 / value,
                              "poisson_rel_err_vs_fp64": perr,
                              "poisson_vcycles_per_step": st32.poisson_iterations / args.steps},
+            "adjoint": adj,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

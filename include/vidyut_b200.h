@@ -240,6 +240,39 @@ vd_status vd_profile_read(void* ctx, long long* launches, double* total_ms,
  * vd_create when ctx is NULL). */
 vd_status vd_last_error(void* ctx, char* buf, int len);
 
+/* Discrete adjoint of N explicit flux + source steps.  No counterpart in the
+ * reference (which has no sensitivities); it differentiates this map of the
+ * transported (non-background) species u, from the current state:
+ *   u <- u + dt ( -div F(u; p_mob) + N_A wdot(u; theta) )
+ * F the drift flux of vd_explicit_rhs's schemes (hyp_order, weno_scheme)
+ * with v = mu(Te, n_total, |E|) E, the electron mobility times p_mob; ghost
+ * cells by clamping (periodic wrap where periodic), zero flux on IHNEUBC and
+ * AXISBC walls; E, Te and the background species frozen at the current
+ * state; wdot the case's mechanism with every pre-factor A_r multiplied by
+ * exp(theta_r).  The state itself is not changed.
+ * Objective VD_ADJ_OBJ_ELECTRONS: total electron count sum n_e dV after the
+ * last step.  Parameters: theta_0 .. theta_{R-1} (R = reactions), then
+ * p_mob; defaults 0 and 1.
+ *   vd_adjoint_num_params   R + 1, or 0 when the case's mechanism has no
+ *                           differentiable form (the adjoint calls then
+ *                           return VD_ERR_UNSUPPORTED);
+ *   vd_adjoint_forward      the objective after nsteps steps; species_out
+ *                           (optional, host) receives the final u, one
+ *                           component of N cells after another in component
+ *                           order;
+ *   vd_adjoint_run          objective and gradient (n_params entries):
+ *                           forward with a device checkpoint every K steps,
+ *                           backward with each K-block recomputed from its
+ *                           checkpoint ((nsteps/K + max(K,2)) state copies
+ *                           of device memory). */
+#define VD_ADJ_OBJ_ELECTRONS 0
+vd_status vd_adjoint_num_params(void* ctx, int* n_params);
+vd_status vd_adjoint_set_params(void* ctx, const double* params, int n_params);
+vd_status vd_adjoint_forward(void* ctx, int nsteps, int objective_id, double* objective,
+                             double* species_out);
+vd_status vd_adjoint_run(void* ctx, int nsteps, int K, int objective_id, double* objective,
+                         double* grad_out, int n_params);
+
 /* Poisson solve that allocates no device memory.  No counterpart in the
  * reference: it serves callers that must not allocate device memory while
  * they run, e.g. a host framework whose own memory pool owns the whole

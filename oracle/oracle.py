@@ -42,6 +42,8 @@ def load(case: str) -> C.CDLL:
         "vdo_poisson_solve": [P, C.c_double, C.POINTER(vb.vd_solve_stats)],
         "vdo_explicit_rhs": [P, C.c_double, P],
         "vdo_implicit_diffusion": [P, C.c_int, C.c_double, P, C.POINTER(vb.vd_solve_stats)],
+        "vdo_adjoint_tlm": [P, C.c_int, C.POINTER(C.c_double), C.c_int,
+                            C.POINTER(C.c_double), C.POINTER(C.c_double), P],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -118,3 +120,21 @@ class Oracle:
         st = vb.vd_solve_stats()
         self.lib.vdo_implicit_diffusion(self.ctx, specid, time, _ptr(a), C.byref(st))
         return st
+
+    def adjoint_tlm(self, nsteps: int, params, species: bool = False):
+        """Objective and gradient of the library's adjoint forward map by an
+        FP64 tangent-linear pass (all parameter directions at once)."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        g = np.zeros(p.size)
+        J = C.c_double()
+        out = None
+        if species:
+            nt = self.info["num_species"] - int(self.cfg.c.num_bg_species)
+            out = np.empty((nt, self.shape[2], self.shape[1], self.shape[0]))
+        dp = C.POINTER(C.c_double)
+        st = self.lib.vdo_adjoint_tlm(self.ctx, nsteps, p.ctypes.data_as(dp), p.size,
+                                      C.byref(J), g.ctypes.data_as(dp),
+                                      _ptr(out) if out is not None else None)
+        if st != 0:
+            raise RuntimeError(f"vdo_adjoint_tlm failed with status {st}")
+        return (J.value, g, out) if species else (J.value, g)

@@ -1656,3 +1656,239 @@ int vdo_implicit_diffusion(void* ctx, int spec, double time, const double* expl_
 }
 
 } // extern "C"
+
+// ============================================ tangent-linear adjoint check
+// FP64 tangent-linear restatement of the forward map the library's discrete
+// adjoint differentiates (declared with vd_adjoint_run): explicit drift flux
+// and mechanism source steps of the transported species, E, Te and the
+// background species frozen, ghost cells by clamping (periodic wrap), zero
+// flux on IHNEUBC/AXISBC walls.  Every value carries its derivatives with
+// respect to the NUM_REACTIONS log pre-factor shifts and the electron
+// mobility scale as dual-number directions, so one forward pass gives the
+// objective and its whole gradient.
+#ifdef VD_HAS_MECH_ADJOINT
+#include "vd_dual.H"
+
+namespace {
+
+constexpr int TLM_NP = NUM_REACTIONS + 1;
+using TD = vd::Dual<TLM_NP>;
+
+// Source/compute_explicit_flux.H:16-214 on dual numbers (same branches as
+// o_weno / o_waf / o_upwind above).
+TD t_weno(const TD& a, const TD& b, const TD& c, const TD& d, const TD& e, int scheme)
+{
+    using vd::fabs;
+    const Real eps = 1e-20;
+    const TD p1 = (1.0 / 3.0) * a - (7.0 / 6.0) * b + (11.0 / 6.0) * c;
+    const TD p2 = -(1.0 / 6.0) * b + (5.0 / 6.0) * c + (1.0 / 3.0) * d;
+    const TD p3 = (1.0 / 3.0) * c + (5.0 / 6.0) * d - (1.0 / 6.0) * e;
+    const TD t1 = a - 2.0 * b + c, t1b = a - 4.0 * b + 3.0 * c;
+    const TD t2 = b - 2.0 * c + d, t2b = b - d;
+    const TD t3 = c - 2.0 * d + e, t3b = 3.0 * c - 4.0 * d + e;
+    const TD b1 = (13.0 / 12.0) * t1 * t1 + 0.25 * t1b * t1b;
+    const TD b2 = (13.0 / 12.0) * t2 * t2 + 0.25 * t2b * t2b;
+    const TD b3 = (13.0 / 12.0) * t3 * t3 + 0.25 * t3b * t3b;
+    const Real g1 = 0.1, g2 = 0.6, g3 = 0.3;
+    TD a1, a2, a3;
+    if (scheme == 1 || scheme == 2)
+    {
+        a1 = g1 / ((b1 + eps) * (b1 + eps));
+        a2 = g2 / ((b2 + eps) * (b2 + eps));
+        a3 = g3 / ((b3 + eps) * (b3 + eps));
+        if (scheme == 2)
+        {
+            const TD sm = a1 + a2 + a3;
+            const TD w1 = a1 / sm, w2 = a2 / sm, w3 = a3 / sm;
+            auto gk = [](const TD& w, Real g) {
+                return w * (g + g * g - 3.0 * g * w + w * w) / (g * g + w * (1 - 2.0 * g));
+            };
+            a1 = gk(w1, g1);
+            a2 = gk(w2, g2);
+            a3 = gk(w3, g3);
+        }
+    } else
+    {
+        const TD tau = fabs(b1 - b3);
+        const TD r1 = tau / (b1 + eps), r2 = tau / (b2 + eps), r3 = tau / (b3 + eps);
+        a1 = g1 * (1.0 + r1 * r1);
+        a2 = g2 * (1.0 + r2 * r2);
+        a3 = g3 * (1.0 + r3 * r3);
+    }
+    const TD sm = a1 + a2 + a3;
+    return (a1 / sm) * p1 + (a2 / sm) * p2 + (a3 / sm) * p3;
+}
+
+// Face flux from the six cells face-3 .. face+2.
+TD t_flux(const TD* u, const TD* v, int hyp_order, int scheme, Real dxmin, Real dt)
+{
+    using vd::fabs;
+    if (hyp_order == 1)
+    {
+        const Real sgn = std::copysign(1.0, 0.5 * (v[2].v + v[3].v));
+        return u[2] * v[2] * 0.5 * (1.0 + sgn) + u[3] * v[3] * 0.5 * (1.0 - sgn);
+    }
+    if (hyp_order == 2)
+    {
+        const TD vm = 0.5 * (v[2] + v[3]);
+        const Real sgn = std::copysign(1.0, vm.v);
+        const TD cc = vm * dt / dxmin;
+        const TD fL = u[2] * v[2], fR = u[3] * v[3];
+        const TD dl = u[2] - u[1], dm = u[3] - u[2], dr = u[4] - u[3];
+        const TD r = (cc.v >= 0.0) ? dl / (dm + 1.0e-30) : dr / (dm + 1.0e-30);
+        TD lim;
+        if (r.v <= 0.0)
+            lim = TD(1.0);
+        else if (r.v <= 1.0)
+            lim = 1.0 - (1.0 - fabs(cc)) * r;
+        else
+            lim = fabs(cc);
+        return 0.5 * (fL + fR) - 0.5 * sgn * lim * (fR - fL);
+    }
+    TD f[6];
+    for (int m = 0; m < 6; ++m) f[m] = u[m] * v[m];
+    const TD alpha = fabs(0.5 * (v[2] + v[3]));
+    const TD fph = t_weno(f[0], f[1], f[2], f[3], f[4], scheme);
+    const TD fmh = t_weno(f[5], f[4], f[3], f[2], f[1], scheme);
+    const TD uph = t_weno(u[0], u[1], u[2], u[3], u[4], scheme);
+    const TD umh = t_weno(u[5], u[4], u[3], u[2], u[1], scheme);
+    return 0.5 * (fph + alpha * uph) + 0.5 * (fmh - alpha * umh);
+}
+
+} // namespace
+#endif
+
+extern "C" {
+
+// Objective (sum of n_e dV after nsteps) and its gradient with respect to
+// (theta_0 .. theta_{R-1}, electron mobility scale) = params; species_out
+// (optional) receives the final transported species, component by component.
+int vdo_adjoint_tlm(void* ctx, int nsteps, const double* params, int n_params, double* J,
+                    double* grad, double* species_out)
+{
+#ifndef VD_HAS_MECH_ADJOINT
+    (void)ctx; (void)nsteps; (void)params; (void)n_params; (void)J; (void)grad;
+    (void)species_out;
+    return VD_ERR_UNSUPPORTED;
+#else
+    auto* c = static_cast<OCtx*>(ctx);
+    if (n_params != TLM_NP) return VD_ERR_INVALID_ARG;
+    const Geom& geo = c->geo;
+    const long long N = geo.ncell();
+    const Real* S = c->phi_new.d.data();
+    std::vector<int> spec;
+    int eslot = -1;
+    for (int sp = 0; sp < NUM_SPECIES; ++sp)
+        if (!is_bg(*c, sp))
+        {
+            if (sp == c->E_IDX) eslot = (int)spec.size();
+            spec.push_back(sp);
+        }
+    const int nt = (int)spec.size();
+    if (eslot < 0) return VD_ERR_INVALID_ARG;
+    std::vector<Real> th(params, params + NUM_REACTIONS);
+    const TD scale = TD::var(params[NUM_REACTIONS], NUM_REACTIONS);
+    const Real dt = c->cfg.dt, Tg = c->cfg.gas_temperature;
+    Real dxmin = geo.dx[0];
+    for (int d = 1; d < geo.dim; ++d) dxmin = std::min(dxmin, geo.dx[d]);
+    std::vector<int> wlo(nt * 3), whi(nt * 3);
+    for (int s = 0; s < nt; ++s)
+        for (int d = 0; d < 3; ++d)
+        {
+            const int lo = bc_lo_for(*c, spec[s])[d], hi = bc_hi_for(*c, spec[s])[d];
+            wlo[s * 3 + d] = !geo.per[d] && (lo == IHNEUBC || lo == AXISBC);
+            whi[s * 3 + d] = !geo.per[d] && (hi == IHNEUBC || hi == AXISBC);
+        }
+    auto cidx = [&](int i, int j, int k) {
+        int q[3] = {i, j, k};
+        for (int a = 0; a < 3; ++a)
+        {
+            const int n = geo.n[a];
+            if (q[a] < 0) q[a] = geo.per[a] ? ((q[a] % n) + n) % n : 0;
+            if (q[a] >= n) q[a] = geo.per[a] ? q[a] % n : n - 1;
+        }
+        return q[0] + (long long)geo.n[0] * (q[1] + (long long)geo.n[1] * q[2]);
+    };
+    std::vector<TD> u((size_t)nt * N), un((size_t)nt * N), mu((size_t)nt * N);
+    for (int s = 0; s < nt; ++s)
+        for (long long q = 0; q < N; ++q) u[s * N + q] = TD(S[spec[s] * N + q]);
+    for (int step = 0; step < nsteps; ++step)
+    {
+#pragma omp parallel for
+        for (long long q = 0; q < N; ++q)
+        {
+            const Real ex = S[EFX_ID * N + q], ey = S[EFY_ID * N + q], ez = S[EFZ_ID * N + q];
+            const Real em = std::sqrt(ex * ex + ey * ey + ez * ez);
+            TD nd(0.0);
+            int slot = 0;
+            for (int sp = 0; sp < NUM_SPECIES; ++sp)
+            {
+                if (slot < nt && spec[slot] == sp)
+                    nd += u[(slot++) * N + q];
+                else
+                    nd += TD(S[sp * N + q]);
+            }
+            for (int s = 0; s < nt; ++s)
+            {
+                TD m = specMob_T<TD>(spec[s], TD(S[ETEMP_ID * N + q]), nd, TD(em), Tg);
+                if (s == eslot) m = m * scale;
+                mu[s * N + q] = m;
+            }
+        }
+#pragma omp parallel for
+        for (long long q = 0; q < N; ++q)
+        {
+            const int ci[3] = {(int)(q % geo.n[0]), (int)((q / geo.n[0]) % geo.n[1]),
+                               (int)(q / ((long long)geo.n[0] * geo.n[1]))};
+            TD C[NUM_SPECIES], rq[NUM_REACTIONS], W[NUM_SPECIES];
+            int slot = 0;
+            for (int sp = 0; sp < NUM_SPECIES; ++sp)
+            {
+                if (slot < nt && spec[slot] == sp)
+                    C[sp] = u[(slot++) * N + q] / N_A;
+                else
+                    C[sp] = TD(S[sp * N + q] / N_A);
+            }
+            mech_rates<TD>(Tg, C, S[ETEMP_ID * N + q], th.data(), rq);
+            for (int r = 0; r < NUM_REACTIONS; ++r) rq[r].d[r] += rq[r].v; // dq_r/dtheta_r
+            mech_wdot<TD>(rq, W);
+            for (int s = 0; s < nt; ++s)
+            {
+                TD acc(0.0);
+                for (int d = 0; d < geo.dim; ++d)
+                {
+                    TD uu[7], vv[7];
+                    for (int m = 0; m < 7; ++m)
+                    {
+                        int cc[3] = {ci[0], ci[1], ci[2]};
+                        cc[d] += m - 3;
+                        const long long qq = cidx(cc[0], cc[1], cc[2]);
+                        uu[m] = u[s * N + qq];
+                        vv[m] = mu[s * N + qq] * S[(EFX_ID + d) * N + qq];
+                    }
+                    TD flo = t_flux(uu, vv, c->cfg.hyp_order, c->cfg.weno_scheme, dxmin, dt);
+                    TD fhi = t_flux(uu + 1, vv + 1, c->cfg.hyp_order, c->cfg.weno_scheme, dxmin, dt);
+                    if (ci[d] == 0 && wlo[s * 3 + d]) flo = TD(0.0);
+                    if (ci[d] == geo.n[d] - 1 && whi[s * 3 + d]) fhi = TD(0.0);
+                    acc += (flo - fhi) / geo.dx[d];
+                }
+                un[s * N + q] = u[s * N + q] + dt * (acc + W[spec[s]] * N_A);
+            }
+        }
+        u.swap(un);
+    }
+    Real dv = 1.0;
+    for (int d = 0; d < geo.dim; ++d) dv *= geo.dx[d];
+    TD tot(0.0);
+    for (long long q = 0; q < N; ++q) tot += u[eslot * N + q];
+    tot = tot * dv;
+    if (J) *J = tot.v;
+    if (grad)
+        for (int k = 0; k < TLM_NP; ++k) grad[k] = tot.d[k];
+    if (species_out)
+        for (size_t i = 0; i < u.size(); ++i) species_out[i] = u[i].v;
+    return VD_OK;
+#endif
+}
+
+} // extern "C"

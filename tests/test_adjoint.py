@@ -1,0 +1,237 @@
+"""Discrete adjoint of N explicit flux + source steps (no reference
+counterpart; the reference computes no sensitivities).
+
+Objective: total electron count after the last step.  Parameters: the 30
+log pre-factor shifts of the LMEA mechanism and the electron mobility scale.
+Checks, all FP64:
+* the oracle's tangent-linear pass against central differences of its own
+  forward map (CPU);
+* the library's forward map against the oracle's, species by species
+  (relative L2 <= 1e-12, pointwise FP64 arithmetic on both sides);
+* the library's adjoint gradient against the oracle's tangent-linear
+  gradient (<= 1e-9 relative: both are exact derivatives of the same map and
+  differ by rounding only);
+* the library's adjoint gradient against central finite differences of the
+  library's own forward map: |g - fd| <= 1e-6 |fd| + 4 eps |J| / h.  The
+  second term is the differences' own rounding floor (J(p +- h) each carry
+  a relative rounding error of order eps = 2.2e-16); where the objective
+  moves by only ~1e-4 of itself per unit parameter, as in these short runs,
+  that floor is comparable to 1e-6 of the gradient at h = 1e-6, so the small
+  cases use h = 1e-3 (truncation error h^2/6 of the third derivative, ~2e-7
+  relative for the exponential pre-factor dependence) and the 128^3 workload
+  uses h = 1e-6 (relative for the mobility scale, absolute for the log
+  pre-factors);
+* checkpoint intervals that do and do not divide the step count give the same
+  gradient; the same checks through a torch.autograd.Function wrapper (test
+  harness only).
+"""
+import numpy as np
+import pytest
+
+import vidyut_b200 as vb
+from oracle.oracle import Oracle
+from vidyut_b200 import workloads as W
+
+NR = 30
+
+
+def small_case(n=12, seed=3, dt=5e-12):
+    """A box of 0.2 mm so that the drift moves the electrons by a visible
+    fraction of a cell within a few steps (CFL ~ 0.2 per step at 5 MV/m)."""
+    cfg = W.adjoint_config(n, prob_hi=[2e-4, 2e-4, 2e-4], dt=dt)
+    S = W.adjoint_state(cfg, seed, efield=5e6)
+    return cfg, S
+
+
+def params(seed=0):
+    rng = np.random.default_rng(seed)
+    p = np.zeros(NR + 1)
+    p[:NR] = rng.uniform(-0.2, 0.2, NR)
+    p[NR] = 1.1
+    return p
+
+
+def unit(k):
+    e = np.zeros(NR + 1)
+    e[k] = 1.0
+    return e
+
+
+EPS = np.finfo(np.float64).eps
+
+
+def fd_ok(g, fd, J, h):
+    return abs(g - fd) <= 1e-6 * abs(fd) + 4 * EPS * abs(J) / h
+
+
+def grad_close(g, ref, rtol):
+    floor = 1e-6 * np.max(np.abs(ref))
+    err = np.abs(g - ref) / np.maximum(np.abs(ref), floor)
+    return float(np.max(err)), err
+
+
+def test_oracle_tlm_vs_fd():
+    cfg, S = small_case(n=8)
+    o = Oracle(cfg)
+    o.set_state(0, S)
+    p = params()
+    nsteps = 4
+    J, g = o.adjoint_tlm(nsteps, p)
+    assert np.isfinite(J) and J > 0
+    h = 1e-3
+    # the three largest pre-factor sensitivities and the mobility scale
+    ks = list(np.argsort(-np.abs(g[:NR]))[:3]) + [NR]
+    for k in ks:
+        step = h * (p[k] if k == NR else 1.0)
+        Jp, _ = o.adjoint_tlm(nsteps, p + step * unit(k))
+        Jm, _ = o.adjoint_tlm(nsteps, p - step * unit(k))
+        fd = (Jp - Jm) / (2 * step)
+        assert fd_ok(g[k], fd, J, step), (k, fd, g[k])
+    # the mobility scale must matter in this set-up (the flux adjoint is exercised)
+    assert abs(g[NR]) > 1e-8 * J
+
+
+@pytest.mark.gpu
+def test_adjoint_forward_parity(require_gpu):
+    cfg, S = small_case()
+    g = vb.Vidyut(cfg)
+    o = Oracle(cfg)
+    g.set_state(0, S)
+    o.set_state(0, S)
+    p = params()
+    g.adjoint_set_params(p)
+    nsteps = 6
+    Jg, ug = g.adjoint_forward(nsteps, species=True)
+    Jo, _, uo = o.adjoint_tlm(nsteps, p, species=True)
+    assert abs(Jg - Jo) <= 1e-12 * abs(Jo)
+    for s in range(uo.shape[0]):
+        d = np.sqrt(np.mean((ug[s] - uo[s]) ** 2)) / np.sqrt(np.mean(uo[s] ** 2))
+        assert d <= 1e-12, (s, d)
+    # the state itself is untouched
+    np.testing.assert_array_equal(g.get_state(0, 8), S[:8])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("hyp_order,weno", [(5, 3), (5, 1), (5, 2), (2, 3), (1, 3)])
+def test_adjoint_vs_tlm(require_gpu, hyp_order, weno):
+    cfg, S = small_case()
+    cfg["hyp_order"] = hyp_order
+    cfg["weno_scheme"] = weno
+    g = vb.Vidyut(cfg)
+    o = Oracle(cfg)
+    g.set_state(0, S)
+    o.set_state(0, S)
+    p = params(1)
+    g.adjoint_set_params(p)
+    nsteps = 7
+    Jg, gg = g.adjoint_run(nsteps, K=3)
+    Jo, go = o.adjoint_tlm(nsteps, p)
+    assert abs(Jg - Jo) <= 1e-12 * abs(Jo)
+    worst, _ = grad_close(gg, go, 1e-9)
+    assert worst <= 1e-9, worst
+
+
+@pytest.mark.gpu
+def test_adjoint_checkpoint_intervals(require_gpu):
+    cfg, S = small_case()
+    g = vb.Vidyut(cfg)
+    g.set_state(0, S)
+    g.adjoint_set_params(params(2))
+    ref = None
+    for K in (1, 2, 3, 10, 25):
+        J, gr = g.adjoint_run(10, K=K)
+        if ref is None:
+            ref = (J, gr)
+        else:
+            assert abs(J - ref[0]) <= 1e-13 * abs(ref[0])
+            worst, _ = grad_close(gr, ref[1], 1e-12)
+            assert worst <= 1e-12, (K, worst)
+
+
+def fd_gradient(g, p, nsteps, ks, h):
+    out = {}
+    for k in ks:
+        step = h * (p[k] if k == NR else 1.0)
+        g.adjoint_set_params(p + step * unit(k))
+        Jp = g.adjoint_forward(nsteps)
+        g.adjoint_set_params(p - step * unit(k))
+        Jm = g.adjoint_forward(nsteps)
+        out[k] = (Jp - Jm) / (2 * step)
+    g.adjoint_set_params(p)
+    return out
+
+
+@pytest.mark.gpu
+def test_adjoint_vs_fd_small(require_gpu):
+    cfg, S = small_case()
+    g = vb.Vidyut(cfg)
+    g.set_state(0, S)
+    p = params(4)
+    g.adjoint_set_params(p)
+    nsteps = 10
+    J, gr = g.adjoint_run(nsteps, K=4)
+    h = 1e-3
+    fd = fd_gradient(g, p, nsteps, range(NR + 1), h=h)
+    for k in range(NR + 1):
+        assert fd_ok(gr[k], fd[k], J, h * (p[k] if k == NR else 1.0)), (k, gr[k], fd[k])
+
+
+@pytest.mark.gpu
+def test_adjoint_c4_vs_fd(require_gpu):
+    """The 128^3 workload: 50 steps at dt = 1e-12 s, checkpoints every 10;
+    central differences on the four largest pre-factor sensitivities, one
+    small one, and the mobility scale."""
+    cfg = W.adjoint_config(128)
+    S = W.adjoint_state(cfg, 0)
+    g = vb.Vidyut(cfg)
+    g.set_state(0, S)
+    p = np.zeros(NR + 1)
+    p[NR] = 1.0
+    g.adjoint_set_params(p)
+    J, gr = g.adjoint_run(50, K=10)
+    assert np.all(np.isfinite(gr)) and J > 0
+    order = np.argsort(-np.abs(gr[:NR]))
+    ks = list(order[:4]) + [int(order[12]), NR]
+    h = 1e-6
+    fd = fd_gradient(g, p, 50, ks, h=h)
+    for k in ks:
+        assert fd_ok(gr[k], fd[k], J, h), (k, gr[k], fd[k])
+
+
+@pytest.mark.gpu
+def test_adjoint_autograd_wrapper(require_gpu):
+    """torch.autograd.Function over the C ABI (test harness only)."""
+    import torch
+
+    cfg, S = small_case()
+    g = vb.Vidyut(cfg)
+    g.set_state(0, S)
+    nsteps = 5
+
+    class ElectronCount(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, theta, scale):
+            p = np.concatenate([theta.detach().cpu().numpy(),
+                                [float(scale.detach().cpu())]]).astype(np.float64)
+            g.adjoint_set_params(p)
+            J, gr = g.adjoint_run(nsteps, K=2)
+            ctx.save_for_backward(torch.from_numpy(gr))
+            return torch.tensor(J, dtype=torch.float64)
+
+        @staticmethod
+        def backward(ctx, gout):
+            (gr,) = ctx.saved_tensors
+            return gout * gr[:NR], gout * gr[NR]
+
+    theta = torch.zeros(NR, dtype=torch.float64, requires_grad=True)
+    scale = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    J = ElectronCount.apply(theta, scale)
+    (2.0 * J).backward()
+    p = np.zeros(NR + 1)
+    p[NR] = 1.0
+    g.adjoint_set_params(p)
+    h = 1e-3
+    fd = fd_gradient(g, p, nsteps, [NR, int(torch.argmax(theta.grad.abs()))], h=h)
+    for k, ref in fd.items():
+        got = float(scale.grad) if k == NR else float(theta.grad[k])
+        assert fd_ok(got / 2.0, ref, float(J), h), (k, got, ref)

@@ -173,3 +173,37 @@ def test_init_domain_matches_oracle(require_gpu):
     g, o = pair(cfg, prob=prob)
     assert np.array_equal(g.get_state(0, 5), o.get_state(0, 5)) or \
         rel(g.get_state(0, 1), o.get_state(0, 1)) < 1e-14
+
+
+def lmea(n, **kw):
+    cfg = W.lmea_config(n)
+    for k, v in {**TIGHT, **kw}.items():
+        cfg[k] = v
+    return cfg
+
+
+def test_lmea_explicit_rhs_parity(require_gpu):
+    # 8 species + electron energy: four component groups in the explicit
+    # kernel, 30-reaction chemistry with energy exchange
+    cfg = lmea(24)
+    g, o = pair(cfg, W.lmea_state(cfg, 7))
+    o.solve_potential(0.0)
+    g.set_state(0, o.get_state())
+    eg, eo = g.explicit_rhs(0.0), o.explicit_rhs(0.0)
+    for c in [0, 1, 2, 3, 4, 5, 7, 8]:
+        assert rel(eg[c], eo[c]) < 1e-12, (c, rel(eg[c], eo[c]))
+
+
+def test_lmea_step_parity_energy_equation(require_gpu):
+    cfg = lmea(24)
+    g, o = pair(cfg, W.lmea_state(cfg, 8))
+    info = g.info
+    for s in range(2):
+        g.step(1)
+        o.step(1)
+        Sg, So = g.get_state(), o.get_state()
+        for c in [0, 1, 3, 5, 7, info["een_id"], info["etemp_id"], info["pot_id"],
+                  info["ejh_id"], info["eih_id"]]:
+            r = rel(Sg[c], So[c])
+            assert r < 1e-11, (s, c, r)
+        assert Sg[:8].min() >= cfg["min_species_density"]

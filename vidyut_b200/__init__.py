@@ -95,8 +95,11 @@ EXPORTS = [
     "vd_init_domain", "vd_set_state", "vd_get_state", "vd_set_time", "vd_get_time",
     "vd_step", "vd_poisson_solve", "vd_explicit_rhs", "vd_implicit_diffusion",
     "vd_check_state", "vd_launch_count", "vd_profile_kernel", "vd_profile_read",
-    "vd_last_error", "vd_poisson_solve_noalloc",
+    "vd_last_error", "vd_poisson_solve_noalloc", "vd_adjoint_num_params",
+    "vd_adjoint_set_params", "vd_adjoint_forward", "vd_adjoint_run",
 ]
+
+VD_ADJ_OBJ_ELECTRONS = 0
 
 VD_PROF_NONE = 0
 VD_PROF_POISSON_SMOOTH = 1
@@ -151,6 +154,11 @@ def load(case: str) -> C.CDLL:
                                      C.POINTER(C.c_double), C.POINTER(C.c_double), P, P,
                                      C.c_double, C.c_double, C.c_int,
                                      C.POINTER(vd_solve_stats), C.c_char_p, C.c_int],
+        "vd_adjoint_num_params": [P, C.POINTER(C.c_int)],
+        "vd_adjoint_set_params": [P, C.POINTER(C.c_double), C.c_int],
+        "vd_adjoint_forward": [P, C.c_int, C.c_int, C.POINTER(C.c_double), P],
+        "vd_adjoint_run": [P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double),
+                           C.POINTER(C.c_double), C.c_int],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -345,6 +353,49 @@ class Vidyut:
         self._chk(self.lib.vd_profile_read(self.ctx, C.byref(n), C.byref(ms), C.byref(b)),
                   "vd_profile_read")
         return n.value, ms.value, b.value
+
+    def write_plotfile(self, path: str) -> None:
+        """The full state as an AMReX plotfile (Source/Plot.cpp:32-44 layout)."""
+        from .plotfile import var_names, write_plotfile
+        c = self.cfg.c
+        t, step = self.time()
+        write_plotfile(path, self.get_state(), var_names(self.info["names"]),
+                       list(c.prob_lo), list(c.prob_hi), t, step, self.dim)
+
+    # -- discrete adjoint of explicit flux + source steps (no reference counterpart)
+    def adjoint_num_params(self) -> int:
+        n = C.c_int()
+        self._chk(self.lib.vd_adjoint_num_params(self.ctx, C.byref(n)), "vd_adjoint_num_params")
+        return n.value
+
+    def adjoint_set_params(self, params) -> None:
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        self._chk(self.lib.vd_adjoint_set_params(
+            self.ctx, p.ctypes.data_as(C.POINTER(C.c_double)), p.size), "vd_adjoint_set_params")
+
+    def adjoint_forward(self, nsteps: int, species: bool = False,
+                        objective: int = VD_ADJ_OBJ_ELECTRONS):
+        """Objective after `nsteps` steps of the adjoint's forward map (and the
+        final transported species, (nt, nz, ny, nx), when `species`)."""
+        J = C.c_double()
+        out = None
+        if species:
+            nt = self.info["num_species"] - int(self.cfg.c.num_bg_species)
+            out = np.empty((nt, self.shape[2], self.shape[1], self.shape[0]))
+        self._chk(self.lib.vd_adjoint_forward(self.ctx, nsteps, objective, C.byref(J),
+                                              _ptr(out) if out is not None else None),
+                  "vd_adjoint_forward")
+        return (J.value, out) if species else J.value
+
+    def adjoint_run(self, nsteps: int, K: int, objective: int = VD_ADJ_OBJ_ELECTRONS):
+        """(objective, gradient) by the checkpointed backward sweep."""
+        n = self.adjoint_num_params()
+        g = np.zeros(n)
+        J = C.c_double()
+        self._chk(self.lib.vd_adjoint_run(self.ctx, nsteps, K, objective, C.byref(J),
+                                          g.ctypes.data_as(C.POINTER(C.c_double)), n),
+                  "vd_adjoint_run")
+        return J.value, g
 
     def launch_count(self) -> int:
         n = C.c_longlong()

@@ -1,0 +1,372 @@
+// Discrete adjoint of N explicit flux + source steps (sm_100a, FP64).
+//
+// Forward map (per step, every transported species s, i.e. every species
+// that is not a background species):
+//     u_s <- u_s + dt * ( sum_d (F_d,lo - F_d,hi)/dx_d + N_A wdot_s(u; theta) )
+// F is the drift flux of the main path (WENO5/WAF/upwind, the formulas of
+// Source/compute_explicit_flux.H:16-214) with cell velocities
+// v = mu_s(Te, n_total, |E|) E_d (electron mobility times the scale p_mob),
+// ghost densities and velocities by clamping to the boundary cell (periodic
+// wrap in periodic directions), and zero flux on walls whose species BC is
+// IHNEUBC or AXISBC.  E and Te are frozen at their values in the state when
+// the run starts; background species are frozen too.  wdot is the case's
+// mechanism with the log pre-factors shifted by theta (A_r -> A_r e^theta_r).
+// Objective J = sum over cells of n_e dV after the last step.
+//
+// Backward step k (lambda = dJ/du^{k+1}, states recomputed from checkpoints):
+//     lambda <- lambda + dt (dR/du)^T lambda,   g <- g + dt (dR/dp)^T lambda
+// evaluated at u^k.  One thread per face differentiates its flux with dual
+// numbers (one pass for the stencil densities, one for the velocities) and
+// scatters w dF/du_m with FP64 atomics, w = dt (lambda_R - lambda_L)/dx.
+// Stencil positions that clamp onto the same boundary cell are seeded as one
+// direction: the WENO smoothness indicators of such a flat sub-stencil are
+// zero only up to rounding, and per-position derivatives of that rounding
+// residue (amplified by 1/(beta + eps)) swamp the true derivative, whereas
+// moving the copies together keeps the residue's derivative exactly zero; the velocities' dependence on the total density goes through
+// dmu/dn (a one-direction dual through the mobility hook); the chemistry
+// Jacobian comes from one-direction dual evaluations of the mechanism per
+// transported species; the pre-factor gradient uses dq_r/dtheta_r = q_r and
+// the mechanism's transposed stoichiometry.
+#pragma once
+
+#include "vd_dual.H"
+#include "vd_kernels.cuh"
+
+namespace vd {
+
+// ---- the flux formulas of vd_flux.cuh on a generic number type
+template <class R>
+__device__ __forceinline__ R weno5_T(const R& a, const R& b, const R& c, const R& d, const R& e,
+                                     int scheme)
+{
+    const double eps = 1e-20;
+    const R p1 = (1.0 / 3.0) * a - (7.0 / 6.0) * b + (11.0 / 6.0) * c;
+    const R p2 = -(1.0 / 6.0) * b + (5.0 / 6.0) * c + (1.0 / 3.0) * d;
+    const R p3 = (1.0 / 3.0) * c + (5.0 / 6.0) * d - (1.0 / 6.0) * e;
+    const R s1 = a - 2.0 * b + c, s1b = a - 4.0 * b + 3.0 * c;
+    const R s2 = b - 2.0 * c + d, s2b = b - d;
+    const R s3 = c - 2.0 * d + e, s3b = 3.0 * c - 4.0 * d + e;
+    const R b1 = (13.0 / 12.0) * s1 * s1 + 0.25 * s1b * s1b;
+    const R b2 = (13.0 / 12.0) * s2 * s2 + 0.25 * s2b * s2b;
+    const R b3 = (13.0 / 12.0) * s3 * s3 + 0.25 * s3b * s3b;
+    R a1, a2, a3;
+    if (scheme == 3)
+    {
+        const R tau = fabs(b1 - b3);
+        const R r1 = tau / (b1 + eps), r2 = tau / (b2 + eps), r3 = tau / (b3 + eps);
+        a1 = 0.1 * (1.0 + r1 * r1);
+        a2 = 0.6 * (1.0 + r2 * r2);
+        a3 = 0.3 * (1.0 + r3 * r3);
+    } else
+    {
+        const R q1 = b1 + eps, q2 = b2 + eps, q3 = b3 + eps;
+        a1 = 0.1 / (q1 * q1);
+        a2 = 0.6 / (q2 * q2);
+        a3 = 0.3 / (q3 * q3);
+        if (scheme == 2)
+        {
+            const R sum = a1 + a2 + a3;
+            const R w1 = a1 / sum, w2 = a2 / sum, w3 = a3 / sum;
+            a1 = w1 * (0.1 + 0.01 - 0.3 * w1 + w1 * w1) / (0.01 + w1 * (1.0 - 0.2));
+            a2 = w2 * (0.6 + 0.36 - 1.8 * w2 + w2 * w2) / (0.36 + w2 * (1.0 - 1.2));
+            a3 = w3 * (0.3 + 0.09 - 0.9 * w3 + w3 * w3) / (0.09 + w3 * (1.0 - 0.6));
+        }
+    }
+    return (a1 * p1 + a2 * p2 + a3 * p3) / (a1 + a2 + a3);
+}
+
+template <class R>
+__device__ __forceinline__ R face_flux_T(const R* u, const R* v, int hyp_order,
+                                         int weno_scheme, double dxmin, double dt)
+{
+    if (hyp_order == 1)
+    {
+        const double sgn = copysign(1.0, 0.5 * (value(v[2]) + value(v[3])));
+        return u[2] * v[2] * (0.5 * (1.0 + sgn)) + u[3] * v[3] * (0.5 * (1.0 - sgn));
+    }
+    if (hyp_order == 2)
+    {
+        const R vm = 0.5 * (v[2] + v[3]);
+        const double sgn = copysign(1.0, value(vm));
+        const R c = vm * dt / dxmin;
+        const R fL = u[2] * v[2], fR = u[3] * v[3];
+        const R dl = u[2] - u[1], dm = u[3] - u[2], dr = u[4] - u[3];
+        const R rr = (value(c) >= 0.0) ? dl / (dm + 1.0e-30) : dr / (dm + 1.0e-30);
+        R lim;
+        if (value(rr) <= 0.0)
+            lim = R(1.0);
+        else if (value(rr) <= 1.0)
+            lim = 1.0 - (1.0 - fabs(c)) * rr;
+        else
+            lim = fabs(c);
+        return 0.5 * (fL + fR) - 0.5 * sgn * lim * (fR - fL);
+    }
+    const R lam = fabs(0.5 * (v[2] + v[3]));
+    const R fph = weno5_T(u[0] * v[0], u[1] * v[1], u[2] * v[2], u[3] * v[3], u[4] * v[4],
+                          weno_scheme);
+    const R fmh = weno5_T(u[5] * v[5], u[4] * v[4], u[3] * v[3], u[2] * v[2], u[1] * v[1],
+                          weno_scheme);
+    const R uph = weno5_T(u[0], u[1], u[2], u[3], u[4], weno_scheme);
+    const R umh = weno5_T(u[5], u[4], u[3], u[2], u[1], weno_scheme);
+    return 0.5 * (fph + lam * uph) + 0.5 * (fmh - lam * umh);
+}
+
+#ifdef VD_HAS_MECH_ADJOINT
+
+struct AdjParams
+{
+    GridDev g; // natural layout
+    double dx[3];
+    double dt, dxmin, Tg, mob_scale;
+    int hyp_order, weno_scheme;
+    int nt;                // transported species
+    int spec[NUM_SPECIES]; // their component indices, ascending
+    int eslot;             // slot of the electrons among them
+    int bclo[NUM_SPECIES][3], bchi[NUM_SPECIES][3];
+    const double* S;     // frozen state: E, Te, background species
+    const double* theta; // log pre-factor shifts (device, NUM_REACTIONS)
+    double* mu;          // nt x N mobilities (times the scale for electrons)
+    double* dmu;         // nt x N d mobility / d total density
+};
+
+__device__ __forceinline__ long long adj_cidx(const GridDev& g, int i, int j, int k)
+{
+    return g.idx(clampi(i, g.n[0], g.per[0]), clampi(j, g.n[1], g.per[1]),
+                 clampi(k, g.n[2], g.per[2]));
+}
+
+__device__ __forceinline__ bool adj_wall(const AdjParams& P, int s, int d, bool hi)
+{
+    return !P.g.per[d] && wall_zero(hi ? P.bchi[s][d] : P.bclo[s][d]);
+}
+
+// Mobilities and their density derivatives of every transported species.
+__global__ void __launch_bounds__(256) k_adj_props(AdjParams P, const double* __restrict__ u)
+{
+    const long long N = P.g.ncell();
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < N;
+         q += (long long)gridDim.x * blockDim.x)
+    {
+        const double ex = P.S[EFX_ID * N + q], ey = P.S[EFY_ID * N + q], ez = P.S[EFZ_ID * N + q];
+        const double em = ::sqrt(ex * ex + ey * ey + ez * ez);
+        const double te = P.S[ETEMP_ID * N + q];
+        double nd = 0.0;
+        int slot = 0;
+        for (int sp = 0; sp < NUM_SPECIES; ++sp)
+        {
+            if (slot < P.nt && P.spec[slot] == sp)
+                nd += u[(slot++) * N + q];
+            else
+                nd += P.S[sp * N + q];
+        }
+        for (int s = 0; s < P.nt; ++s)
+        {
+            const Dual<1> m = specMob_T<Dual<1>>(P.spec[s], Dual<1>(te), Dual<1>::var(nd, 0),
+                                                 Dual<1>(em), P.Tg);
+            const double sc = (s == P.eslot) ? P.mob_scale : 1.0;
+            P.mu[s * N + q] = m.v * sc;
+            P.dmu[s * N + q] = m.d[0] * sc;
+        }
+    }
+}
+
+// One forward step: unew = u + dt R(u).
+__global__ void __launch_bounds__(256) k_adj_step(AdjParams P, const double* __restrict__ u,
+                                                  double* __restrict__ unew)
+{
+    const GridDev& g = P.g;
+    const long long N = g.ncell();
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        int c3[3];
+        cell_of(g, t, c3[0], c3[1], c3[2]);
+        double C[NUM_SPECIES], q[NUM_REACTIONS], W[NUM_SPECIES];
+        int slot = 0;
+        for (int sp = 0; sp < NUM_SPECIES; ++sp)
+        {
+            const bool tr = slot < P.nt && P.spec[slot] == sp;
+            C[sp] = (tr ? u[slot * N + t] : P.S[sp * N + t]) / N_A;
+            if (tr) ++slot;
+        }
+        mech_rates<double>(P.Tg, C, P.S[ETEMP_ID * N + t], P.theta, q);
+        mech_wdot<double>(q, W);
+        for (int s = 0; s < P.nt; ++s)
+        {
+            double acc = 0.0;
+            for (int d = 0; d < g.dim; ++d)
+            {
+                double uu[7], vv[7];
+                for (int m = 0; m < 7; ++m)
+                {
+                    int c[3] = {c3[0], c3[1], c3[2]};
+                    c[d] += m - 3;
+                    const long long qq = adj_cidx(g, c[0], c[1], c[2]);
+                    uu[m] = u[s * N + qq];
+                    vv[m] = P.mu[s * N + qq] * P.S[(EFX_ID + d) * N + qq];
+                }
+                double flo = face_flux6(uu, vv, P.hyp_order, P.weno_scheme, P.dxmin, P.dt);
+                double fhi = face_flux6(uu + 1, vv + 1, P.hyp_order, P.weno_scheme, P.dxmin, P.dt);
+                if (c3[d] == 0 && adj_wall(P, s, d, false)) flo = 0.0;
+                if (c3[d] == g.n[d] - 1 && adj_wall(P, s, d, true)) fhi = 0.0;
+                acc += (flo - fhi) / P.dx[d];
+            }
+            unew[s * N + t] = u[s * N + t] + P.dt * (acc + W[P.spec[s]] * N_A);
+        }
+    }
+}
+
+// Adjoint of the face fluxes of direction d: one thread per face.
+__global__ void __launch_bounds__(128) k_adj_faces(AdjParams P, int d,
+                                                   const double* __restrict__ u,
+                                                   const double* __restrict__ lam,
+                                                   double* __restrict__ adj,
+                                                   double* __restrict__ adjnd, double* gmob)
+{
+    __shared__ double sh[32];
+    const GridDev& g = P.g;
+    const long long N = g.ncell();
+    const int fn[3] = {g.n[0] + (d == 0), g.n[1] + (d == 1), g.n[2] + (d == 2)};
+    const long long nf = (long long)fn[0] * fn[1] * fn[2];
+    double gm = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nf;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        int f3[3];
+        f3[0] = (int)(t % fn[0]);
+        f3[1] = (int)((t / fn[0]) % fn[1]);
+        f3[2] = (int)(t / ((long long)fn[0] * fn[1]));
+        if (g.per[d] && f3[d] == g.n[d]) continue; // the periodic wrap face is face 0
+        // stencil cells; positions that clamp onto the same cell share one
+        // derivative direction (dir[m] = first position of that cell)
+        long long qm[6];
+        int dir[6];
+        for (int m = 0; m < 6; ++m)
+        {
+            int c[3] = {f3[0], f3[1], f3[2]};
+            c[d] += m - 3;
+            qm[m] = adj_cidx(g, c[0], c[1], c[2]);
+            dir[m] = m;
+            for (int q = m - 1; q >= 0; --q)
+                if (qm[q] == qm[m]) dir[m] = dir[q];
+        }
+        const bool hasL = f3[d] > 0 || g.per[d];
+        const bool hasR = f3[d] < g.n[d];
+        for (int s = 0; s < P.nt; ++s)
+        {
+            if (f3[d] == 0 && adj_wall(P, s, d, false)) continue;
+            if (f3[d] == g.n[d] && adj_wall(P, s, d, true)) continue;
+            const double lL = hasL ? lam[s * N + qm[2]] : 0.0;
+            const double lR = hasR ? lam[s * N + qm[3]] : 0.0;
+            const double w = P.dt * (lR - lL) / P.dx[d];
+            if (w == 0.0) continue;
+            double uv[6], vv[6];
+            for (int m = 0; m < 6; ++m)
+            {
+                uv[m] = u[s * N + qm[m]];
+                vv[m] = P.mu[s * N + qm[m]] * P.S[(EFX_ID + d) * N + qm[m]];
+            }
+            {
+                Dual<6> U[6], V[6];
+                for (int m = 0; m < 6; ++m)
+                {
+                    U[m] = Dual<6>::var(uv[m], dir[m]);
+                    V[m] = Dual<6>(vv[m]);
+                }
+                const Dual<6> F = face_flux_T(U, V, P.hyp_order, P.weno_scheme, P.dxmin, P.dt);
+                for (int m = 0; m < 6; ++m)
+                    if (dir[m] == m && F.d[m] != 0.0) atomicAdd(&adj[s * N + qm[m]], w * F.d[m]);
+            }
+            {
+                Dual<6> U[6], V[6];
+                for (int m = 0; m < 6; ++m)
+                {
+                    U[m] = Dual<6>(uv[m]);
+                    V[m] = Dual<6>::var(vv[m], dir[m]);
+                }
+                const Dual<6> F = face_flux_T(U, V, P.hyp_order, P.weno_scheme, P.dxmin, P.dt);
+                for (int m = 0; m < 6; ++m)
+                {
+                    if (dir[m] != m || F.d[m] == 0.0) continue;
+                    const double e = P.S[(EFX_ID + d) * N + qm[m]];
+                    const double dn = P.dmu[s * N + qm[m]] * e;
+                    if (dn != 0.0) atomicAdd(&adjnd[qm[m]], w * F.d[m] * dn);
+                    if (s == P.eslot) gm += w * F.d[m] * vv[m];
+                }
+            }
+        }
+    }
+    gm = block_sum(gm, sh);
+    if (threadIdx.x == 0 && gm != 0.0) atomicAdd(gmob, gm / P.mob_scale);
+}
+
+// Adjoint of the chemistry, then the adjoint update of the step:
+//   lambda_s <- lambda_s + dt (dW/dC)^T lambda + adj_s + adjnd
+// (adj: the flux terms, adjnd: the density term of the mobilities, shared by
+// every transported species since n_total sums them).
+__global__ void __launch_bounds__(128) k_adj_chem_update(AdjParams P,
+                                                         const double* __restrict__ u,
+                                                         double* __restrict__ lam,
+                                                         const double* __restrict__ adj,
+                                                         const double* __restrict__ adjnd,
+                                                         double* gtheta)
+{
+    __shared__ double sh[32];
+    const long long N = P.g.ncell();
+    double gl[NUM_REACTIONS];
+    for (int r = 0; r < NUM_REACTIONS; ++r) gl[r] = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        const double te = P.S[ETEMP_ID * N + t];
+        double Cv[NUM_SPECIES], lamc[NUM_SPECIES];
+        int slot = 0;
+        for (int sp = 0; sp < NUM_SPECIES; ++sp)
+        {
+            const bool tr = slot < P.nt && P.spec[slot] == sp;
+            Cv[sp] = (tr ? u[slot * N + t] : P.S[sp * N + t]) / N_A;
+            lamc[sp] = tr ? lam[slot * N + t] : 0.0;
+            if (tr) ++slot;
+        }
+        // pre-factor gradient: dR_s/dtheta_r = N_A nu_sr q_r
+        {
+            double q[NUM_REACTIONS], ln[NUM_REACTIONS];
+            mech_rates<double>(P.Tg, Cv, te, P.theta, q);
+            mech_lam_nu(lamc, ln);
+            for (int r = 0; r < NUM_REACTIONS; ++r) gl[r] += P.dt * N_A * q[r] * ln[r];
+        }
+        // dR_s/du_s2 = d wdot_s / d C_s2 (R = N_A wdot, C = u / N_A), one column per pass
+        const double nd = adjnd[t];
+        for (int s2 = 0; s2 < P.nt; ++s2)
+        {
+            Dual<1> C[NUM_SPECIES], q[NUM_REACTIONS], W[NUM_SPECIES];
+            for (int sp = 0; sp < NUM_SPECIES; ++sp) C[sp] = Dual<1>(Cv[sp]);
+            C[P.spec[s2]].d[0] = 1.0;
+            mech_rates<Dual<1>>(P.Tg, C, te, P.theta, q);
+            mech_wdot<Dual<1>>(q, W);
+            double a = 0.0;
+            for (int sp = 0; sp < NUM_SPECIES; ++sp) a += lamc[sp] * W[sp].d[0];
+            lam[s2 * N + t] = lamc[P.spec[s2]] + P.dt * a + adj[s2 * N + t] + nd;
+        }
+    }
+    for (int r = 0; r < NUM_REACTIONS; ++r)
+    {
+        const double v = block_sum(gl[r], sh);
+        if (threadIdx.x == 0 && v != 0.0) atomicAdd(&gtheta[r], v);
+    }
+}
+
+#endif // VD_HAS_MECH_ADJOINT
+
+__global__ void k_adj_objective(long long n, const double* __restrict__ ue, double dv, double* J)
+{
+    __shared__ double sh[32];
+    double s = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        s += ue[t];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) atomicAdd(J, s * dv);
+}
+
+} // namespace vd

@@ -2,8 +2,9 @@
 // the local Lax-Friedrichs split, the second-order WAF flux with the MINBEE
 // limiter, and first-order upwind.  Same schemes and constants as the
 // reference (Source/compute_explicit_flux.H:16-214, including the Rathan &
-// Naga Raju WENO-M/Z weights), arranged for FP64 throughput: one reciprocal
-// per weight normalisation instead of three divisions.
+// Naga Raju WENO-M/Z weights), arranged for FP64 throughput: the three
+// 1/(beta_k + eps) from one division of their product, and one division for
+// the weight normalisation (two FP64 divisions per reconstruction, not four).
 #pragma once
 
 namespace vd {
@@ -29,19 +30,34 @@ __device__ __forceinline__ double weno5(double a, double b, double c, double d, 
     const double b2 = (13.0 / 12.0) * s2 * s2 + 0.25 * s2b * s2b;
     const double b3 = (13.0 / 12.0) * s3 * s3 + 0.25 * s3b * s3b;
     double a1, a2, a3;
+    const double q1 = b1 + eps, q2 = b2 + eps, q3 = b3 + eps;
+    // one division for the three 1/q_k when the product is representable
+    const double prod = q1 * q2 * q3;
+    double i1, i2, i3;
+    if (prod < 1e300)
+    {
+        const double ip = 1.0 / prod;
+        i1 = q2 * q3 * ip;
+        i2 = q1 * q3 * ip;
+        i3 = q1 * q2 * ip;
+    } else
+    {
+        i1 = 1.0 / q1;
+        i2 = 1.0 / q2;
+        i3 = 1.0 / q3;
+    }
     if (scheme == 3)
     {
         const double tau = fabs(b1 - b3);
-        const double r1 = tau / (b1 + eps), r2 = tau / (b2 + eps), r3 = tau / (b3 + eps);
+        const double r1 = tau * i1, r2 = tau * i2, r3 = tau * i3;
         a1 = 0.1 * (1.0 + r1 * r1);
         a2 = 0.6 * (1.0 + r2 * r2);
         a3 = 0.3 * (1.0 + r3 * r3);
     } else
     {
-        const double q1 = b1 + eps, q2 = b2 + eps, q3 = b3 + eps;
-        a1 = 0.1 / (q1 * q1);
-        a2 = 0.6 / (q2 * q2);
-        a3 = 0.3 / (q3 * q3);
+        a1 = 0.1 * (i1 * i1);
+        a2 = 0.6 * (i2 * i2);
+        a3 = 0.3 * (i3 * i3);
         if (scheme == 2)
         {
             const double inv = 1.0 / (a1 + a2 + a3);
@@ -82,21 +98,33 @@ __device__ __forceinline__ double upwind_flux(double vL, double vR, double pL, d
     return pL * vL * 0.5 * (1.0 + sgn) + pR * vR * 0.5 * (1.0 - sgn);
 }
 
-// Face flux from the six cells around the face (u[0..5] = cells face-3 ..
-// face+2, v[] their drift velocities).
+// Face flux from the six cells around the face (u0..u5 = cells face-3 ..
+// face+2, v0..v5 their drift velocities).  Kept out of line: a kernel calls it
+// at several sites, and one shared copy keeps the instruction working set
+// small enough for the instruction cache.
+__device__ __noinline__ double face_flux_v(double u0, double u1, double u2, double u3,
+                                           double u4, double u5, double v0, double v1,
+                                           double v2, double v3, double v4, double v5,
+                                           int hyp_order, int weno_scheme, double dxmin,
+                                           double dt)
+{
+    if (hyp_order == 1) return upwind_flux(v2, v3, u2, u3);
+    if (hyp_order == 2) return waf_flux(v2, v3, u1, u2, u3, u4, dxmin, dt);
+    const double f0 = u0 * v0, f1 = u1 * v1, f2 = u2 * v2, f3 = u3 * v3, f4 = u4 * v4,
+                 f5 = u5 * v5;
+    const double lam = fabs(0.5 * (v2 + v3));
+    const double fph = weno5(f0, f1, f2, f3, f4, weno_scheme);
+    const double fmh = weno5(f5, f4, f3, f2, f1, weno_scheme);
+    const double uph = weno5(u0, u1, u2, u3, u4, weno_scheme);
+    const double umh = weno5(u5, u4, u3, u2, u1, weno_scheme);
+    return 0.5 * (fph + lam * uph) + 0.5 * (fmh - lam * umh);
+}
+
 __device__ __forceinline__ double face_flux6(const double* u, const double* v, int hyp_order,
                                              int weno_scheme, double dxmin, double dt)
 {
-    if (hyp_order == 1) return upwind_flux(v[2], v[3], u[2], u[3]);
-    if (hyp_order == 2) return waf_flux(v[2], v[3], u[1], u[2], u[3], u[4], dxmin, dt);
-    const double f0 = u[0] * v[0], f1 = u[1] * v[1], f2 = u[2] * v[2], f3 = u[3] * v[3],
-                 f4 = u[4] * v[4], f5 = u[5] * v[5];
-    const double lam = fabs(0.5 * (v[2] + v[3]));
-    const double fph = weno5(f0, f1, f2, f3, f4, weno_scheme);
-    const double fmh = weno5(f5, f4, f3, f2, f1, weno_scheme);
-    const double uph = weno5(u[0], u[1], u[2], u[3], u[4], weno_scheme);
-    const double umh = weno5(u[5], u[4], u[3], u[2], u[1], weno_scheme);
-    return 0.5 * (fph + lam * uph) + 0.5 * (fmh - lam * umh);
+    return face_flux_v(u[0], u[1], u[2], u[3], u[4], u[5], v[0], v[1], v[2], v[3], v[4], v[5],
+                       hyp_order, weno_scheme, dxmin, dt);
 }
 
 } // namespace vd

@@ -287,44 +287,49 @@ __device__ __forceinline__ double grad_at_face(const GradCtx& C, const double* _
 }
 
 // ---------------- E field, reduced field, potential (Source/PotentialSolve.cpp:500-541)
-__global__ void k_efield(GradCtx C, const double* __restrict__ sol, double* __restrict__ S,
-                         double ps)
+// Grid: (row blocks, ny, nz).  Faces inside the domain are plain differences
+// of the solution; boundary faces go through the solve's closure.
+__global__ void __launch_bounds__(128) k_efield(GradCtx C, const double* __restrict__ sol,
+                                                double* __restrict__ S, double ps)
 {
     const GridDev& g = C.op.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n[0]) return;
+    const int j = blockIdx.y, k = blockIdx.z;
     const long long N = g.ncell();
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
-         t += (long long)gridDim.x * blockDim.x)
-    {
-        int i, j, k;
-        i = (int)(t % g.n[0]);
-        j = (int)((t / g.n[0]) % g.n[1]);
-        k = (int)(t / ((long long)g.n[0] * g.n[1]));
-        double E[3] = {0.0, 0.0, 0.0};
-        for (int d = 0; d < g.dim; ++d)
-        {
-            int p[3] = {i, j, k};
-            p[d] += 1;
-            const double flo = grad_at_face(C, sol, d, i, j, k) * (-1.0 * ps);
-            const double fhi = grad_at_face(C, sol, d, p[0], p[1], p[2]) * (-1.0 * ps);
-            E[d] = 0.5 * (flo + fhi);
-            S[(EFX_ID + d) * N + t] = E[d];
-        }
-        double Esum = 0.0, nd = 0.0;
+    const long long t = i + (long long)g.n[0] * (j + (long long)g.n[1] * k);
+    const double x0 = sol[g.idx(i, j, k)];
+    double E[3] = {0.0, 0.0, 0.0};
+    const int c3[3] = {i, j, k};
 #pragma unroll
-        for (int sp = 0; sp < NUM_SPECIES; sp++) nd += S[sp * N + t];
-        nd = nd - S[E_ID * N + t];
-        for (int d = 0; d < g.dim; ++d) Esum += E[d] * E[d];
-        S[REF_ID * N + t] = (sqrt(Esum) / nd) / 1.0e-21;
-        S[POT_ID * N + t] = sol[g.idx(i, j, k)] * ps;
+    for (int d = 0; d < 3; ++d)
+    {
+        if (d >= g.dim) break;
+        int m[3] = {i, j, k}, p[3] = {i, j, k};
+        m[d] -= 1;
+        p[d] += 1;
+        const double glo = (c3[d] > 0) ? (x0 - sol[g.idx(m[0], m[1], m[2])]) * C.dxi[d]
+                                       : grad_at_face(C, sol, d, i, j, k);
+        const double ghi = (c3[d] < g.n[d] - 1)
+                               ? (sol[g.idx(p[0], p[1], p[2])] - x0) * C.dxi[d]
+                               : grad_at_face(C, sol, d, p[0], p[1], p[2]);
+        E[d] = 0.5 * (glo * (-1.0 * ps) + ghi * (-1.0 * ps));
+        S[(EFX_ID + d) * N + t] = E[d];
     }
+    double Esum = 0.0, nd = 0.0;
+#pragma unroll
+    for (int sp = 0; sp < NUM_SPECIES; sp++) nd += S[sp * N + t];
+    nd = nd - S[E_ID * N + t];
+    for (int d = 0; d < g.dim; ++d) Esum += E[d] * E[d];
+    S[REF_ID * N + t] = (sqrt(Esum) / nd) / 1.0e-21;
+    S[POT_ID * N + t] = x0 * ps;
 }
 
 // ---------------- fused reactions + drift flux + divergence
 // (update_rxnsrc_at_all_levels, Source/ScalarSolve.cpp:181-209;
 //  compute_scalar_transport_flux + compute_flux, Source/ScalarSolve.cpp:285-324,
 //  Source/compute_explicit_flux.H:218-415; compute_dsdt, Source/ScalarSolve.cpp:50-78).
-// Every transported component's explicit source in one pass over the cells;
-// each thread evaluates its cell's low and high faces in every direction.
+// Every transported component's explicit source in one pass over the cells.
 struct ExplParams
 {
     Geo G;
@@ -343,99 +348,280 @@ struct ExplParams
 
 __device__ __forceinline__ bool wall_zero(int code) { return code == IHNEUBC || code == AXISBC; }
 
-__global__ void __launch_bounds__(256) k_explicit(ExplParams P)
+// Streaming form of the same update.  A CTA owns an EX_TX x EX_TY column of
+// cells and marches along z over a chunk of planes.  Each loaded plane
+// (with a 3-cell xy halo) gives, per transported component of the group,
+// n and the x/y drift velocities in shared memory; the x and y face fluxes
+// of that plane are computed once per face.  The z stencil lives in a
+// six-plane register queue per thread, so every z face is also computed
+// once.  Output for plane z happens three planes after it is loaded.  The
+// first group launch evaluates the chemistry once per cell and stores the
+// reaction sources of every component; later group launches (components
+// beyond the first EX_QB) read them back.  Accumulation order per cell is
+// the reference's ((Fx + rxn) + Fy) + Fz.
+#define EX_TX 32
+#define EX_TY 8
+#define EX_HX (EX_TX + 6)
+#define EX_HY (EX_TY + 6)
+#define EX_QB 1
+
+__device__ __forceinline__ void ex_cell_vel(const ExplParams& P, int ci, int cj, int ck,
+                                            int ui, int uj, int uk, int comp, double te,
+                                            double nd, double em, double ex, double ey,
+                                            double ez, double& vx, double& vy, double& vz)
 {
+#ifdef VD_HAS_USER_TRANSPORT
+    if (P.user_vel)
+    {
+        Array4 sv = state_view(const_cast<double*>(P.S), P.G.g);
+        const IntVect c{ui, uj, uk};
+        vx = user_transport::compute_vel(c, 0, comp, sv, ga3(P.G.dx), P.time, *P.pp, P.Tg, P.Pg);
+        vy = (P.G.g.dim > 1) ? user_transport::compute_vel(c, 1, comp, sv, ga3(P.G.dx), P.time,
+                                                            *P.pp, P.Tg, P.Pg)
+                             : 0.0;
+        vz = (P.G.g.dim > 2) ? user_transport::compute_vel(c, 2, comp, sv, ga3(P.G.dx), P.time,
+                                                            *P.pp, P.Tg, P.Pg)
+                             : 0.0;
+        return;
+    }
+#endif
+    const double mu = specMob(comp, te, nd, em, P.Tg);
+    vx = mu * ex;
+    vy = mu * ey;
+    vz = mu * ez;
+}
+
+__global__ void __launch_bounds__(256, 2) k_explicit_stream(ExplParams P, int q0, int zc)
+{
+    __shared__ double s_n[EX_QB][EX_HY][EX_HX];
+    __shared__ double s_vx[EX_QB][EX_HY][EX_HX];
+    __shared__ double s_vy[EX_QB][EX_HY][EX_HX];
+    __shared__ double s_vz[EX_QB][EX_HY][EX_HX];
+    __shared__ double s_fx[EX_QB][EX_TY][EX_TX + 1];
+    __shared__ double s_fy[EX_QB][EX_TY + 1][EX_TX];
     const GridDev& g = P.G.g;
     const long long N = g.ncell();
     const double* __restrict__ S = P.S;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
-         t += (long long)gridDim.x * blockDim.x)
-    {
-        int c3[3];
-        cell_of(g, t, c3[0], c3[1], c3[2]);
-        double rx[VD_NT];
-#pragma unroll
-        for (int q = 0; q < VD_NT; ++q) rx[q] = 0.0;
-        if (P.do_reactions)
-        {
-            double C[NUM_SPECIES], W[NUM_SPECIES];
-#pragma unroll
-            for (int sp = 0; sp < NUM_SPECIES; sp++) C[sp] = S[sp * N + t] / N_A;
-            double ee = 0.0;
-            CKWC(P.Tg, C, W, S[ETEMP_ID * N + t], S[REF_ID * N + t], &ee);
-#pragma unroll
-            for (int sp = 0; sp < NUM_SPECIES; sp++) rx[sp] = W[sp] * N_A;
-            rx[NUM_SPECIES] = ee;
-#ifndef VD_NO_USER_REACT_SOURCES
-            Array4 sv = state_view(const_cast<double*>(S), g);
-            Array4 rv = cell_view(rx, c3[0], c3[1], c3[2]);
-            user_sources::add_user_react_sources(c3[0], c3[1], c3[2], sv, rv, ga3(P.G.plo),
-                                                 ga3(P.G.phi), ga3(P.G.dx), P.time, *P.pp,
-                                                 P.Tg, P.Pg);
-#endif
-        }
-        if (P.rxn_een) P.rxn_een[t] = rx[NUM_SPECIES];
-        for (int sp = 0; sp < NUM_SPECIES; sp++)
-            if (P.bg[sp]) P.expl[sp * N + t] = P.do_bg_rxn ? rx[sp] : 0.0;
+    const int dim = g.dim;
+    const int tx = threadIdx.x % EX_TX, ty = threadIdx.x / EX_TX;
+    const int i0 = blockIdx.x * EX_TX, j0 = blockIdx.y * EX_TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool active = i < g.n[0] && j < g.n[1];
+    const int nq = min(EX_QB, P.ntr - q0);
+    const int zb = blockIdx.z * zc;
+    const int ze = min(zb + zc, g.n[2]);
+    const int lag = (dim == 3) ? 3 : 0;
+    const int pfirst = (dim == 3) ? zb - 3 : zb;
+    const int plast = ze - 1 + lag;
+    const double dxmin = P.dxmin;
 
-        double acc[VD_NT];
-        for (int q = 0; q < P.ntr; ++q) acc[q] = 0.0;
-        for (int d = 0; d < g.dim && P.do_transport; ++d)
-        {
-            // per stencil position: cell index, Te, heavy sum, |E|, E_d
-            long long qi[7];
-            double te[7], nd[7], em[7], ed[7];
-            for (int m = 0; m < 7; ++m)
+    double qn[EX_QB][6], qv[EX_QB][6], qdx[EX_QB][4], qdy[EX_QB][4], fzlo[EX_QB];
+#pragma unroll
+    for (int s = 0; s < EX_QB; ++s)
+    {
+#pragma unroll
+        for (int m = 0; m < 6; ++m) qn[s][m] = qv[s][m] = 0.0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) qdx[s][m] = qdy[s][m] = 0.0;
+        fzlo[s] = 0.0;
+    }
+
+    for (int p = pfirst; p <= plast; ++p)
+    {
+        const int pz = clampi(p, g.n[2], g.per[2]);
+        __syncthreads();
+        // ---- load plane p with its xy halo
+        if (P.do_transport)
+            for (int c = threadIdx.x; c < EX_HX * EX_HY; c += blockDim.x)
             {
-                int c[3] = {c3[0], c3[1], c3[2]};
-                c[d] = clampi(c[d] + m - 3, g.n[d], g.per[d]);
-                const long long q = g.idx(c[0], c[1], c[2]);
-                qi[m] = q;
+                const int hx = c % EX_HX, hy = c / EX_HX;
+                const int ui = i0 + hx - 3, uj = j0 + hy - 3;
+                const int ci = clampi(ui, g.n[0], g.per[0]);
+                const int cj = (dim > 1) ? clampi(uj, g.n[1], g.per[1]) : 0;
+                const long long q = g.idx(ci, cj, pz);
                 const double ex = S[EFX_ID * N + q], ey = S[EFY_ID * N + q],
                              ez = S[EFZ_ID * N + q];
-                em[m] = sqrt(ex * ex + ey * ey + ez * ez);
-                ed[m] = S[(EFX_ID + d) * N + q];
-                te[m] = S[ETEMP_ID * N + q];
-                double s = 0.0;
+                const double em = sqrt(ex * ex + ey * ey + ez * ez);
+                const double te = S[ETEMP_ID * N + q];
+                double nd = 0.0;
 #pragma unroll
-                for (int sp = 0; sp < NUM_SPECIES; sp++) s += S[sp * N + q];
-                nd[m] = s;
+                for (int sp = 0; sp < NUM_SPECIES; sp++) nd += S[sp * N + q];
+#pragma unroll
+                for (int s = 0; s < EX_QB; ++s)
+                {
+                    if (s >= nq) break;
+                    const int comp = P.comp[q0 + s];
+                    double vx, vy, vz;
+                    ex_cell_vel(P, ci, cj, pz, ui, uj, p, comp, te, nd, em, ex, ey, ez, vx, vy,
+                                vz);
+                    s_n[s][hy][hx] = S[comp * N + q];
+                    s_vx[s][hy][hx] = vx;
+                    s_vy[s][hy][hx] = vy;
+                    s_vz[s][hy][hx] = vz;
+                }
             }
-            for (int q = 0; q < P.ntr; ++q)
+        __syncthreads();
+        // ---- x and y face fluxes of plane p
+        if (P.do_transport && active)
+        {
+#pragma unroll
+            for (int s = 0; s < EX_QB; ++s)
             {
-                const int comp = P.comp[q];
+                if (s >= nq) break;
+                const int qc = q0 + s;
                 double u[7], v[7];
+#pragma unroll
                 for (int m = 0; m < 7; ++m)
                 {
-                    u[m] = S[comp * N + qi[m]];
-#ifdef VD_HAS_USER_TRANSPORT
-                    if (P.user_vel)
-                    {
-                        int c[3] = {c3[0], c3[1], c3[2]};
-                        c[d] += m - 3;
-                        Array4 sv = state_view(const_cast<double*>(S), g);
-                        v[m] = user_transport::compute_vel(IntVect{c[0], c[1], c[2]}, d, comp,
-                                                           sv, ga3(P.G.dx), P.time, *P.pp,
-                                                           P.Tg, P.Pg);
-                    } else
-#endif
-                        v[m] = specMob(comp, te[m], nd[m], em[m], P.Tg) * ed[m];
+                    u[m] = s_n[s][ty + 3][tx + m];
+                    v[m] = s_vx[s][ty + 3][tx + m];
                 }
-                double flo = face_flux6(u, v, P.hyp_order, P.weno_scheme, P.dxmin, P.dt);
-                double fhi = face_flux6(u + 1, v + 1, P.hyp_order, P.weno_scheme, P.dxmin, P.dt);
-                if (c3[d] == 0 && wall_zero(P.bclo[q][d])) flo = 0.0;
-                if (c3[d] == g.n[d] - 1 && wall_zero(P.bchi[q][d])) fhi = 0.0;
-                if (d == 0)
-                    acc[q] = (flo - fhi) / P.G.dx[0] + rx[comp];
-                else
-                    acc[q] += (flo - fhi) / P.G.dx[d];
+                double f = face_flux6(u, v, P.hyp_order, P.weno_scheme, dxmin, P.dt);
+                if (i == 0 && wall_zero(P.bclo[qc][0])) f = 0.0;
+                s_fx[s][ty][tx] = f;
+                if (tx == EX_TX - 1 || i == g.n[0] - 1)
+                {
+                    double fh = face_flux6(u + 1, v + 1, P.hyp_order, P.weno_scheme, dxmin, P.dt);
+                    if (i == g.n[0] - 1 && wall_zero(P.bchi[qc][0])) fh = 0.0;
+                    s_fx[s][ty][tx + 1] = fh;
+                }
+                if (dim > 1)
+                {
+#pragma unroll
+                    for (int m = 0; m < 7; ++m)
+                    {
+                        u[m] = s_n[s][ty + m][tx + 3];
+                        v[m] = s_vy[s][ty + m][tx + 3];
+                    }
+                    double fy = face_flux6(u, v, P.hyp_order, P.weno_scheme, dxmin, P.dt);
+                    if (j == 0 && wall_zero(P.bclo[qc][1])) fy = 0.0;
+                    s_fy[s][ty][tx] = fy;
+                    if (ty == EX_TY - 1 || j == g.n[1] - 1)
+                    {
+                        double fh =
+                            face_flux6(u + 1, v + 1, P.hyp_order, P.weno_scheme, dxmin, P.dt);
+                        if (j == g.n[1] - 1 && wall_zero(P.bchi[qc][1])) fh = 0.0;
+                        s_fy[s][ty + 1][tx] = fh;
+                    }
+                }
             }
         }
-        for (int q = 0; q < P.ntr; ++q)
+        __syncthreads();
+        // ---- queues: this plane's x/y divergences and z stencil values
+#pragma unroll
+        for (int s = 0; s < EX_QB; ++s)
         {
-            const int comp = P.comp[q];
-            P.expl[comp * N + t] = P.do_transport ? acc[q] : rx[comp];
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+            {
+                qdx[s][m] = qdx[s][m + 1];
+                qdy[s][m] = qdy[s][m + 1];
+            }
+#pragma unroll
+            for (int m = 0; m < 5; ++m)
+            {
+                qn[s][m] = qn[s][m + 1];
+                qv[s][m] = qv[s][m + 1];
+            }
+            if (s < nq && active && P.do_transport)
+            {
+                qdx[s][3] = (s_fx[s][ty][tx] - s_fx[s][ty][tx + 1]) / P.G.dx[0];
+                qdy[s][3] = (dim > 1) ? (s_fy[s][ty][tx] - s_fy[s][ty + 1][tx]) / P.G.dx[1] : 0.0;
+                qn[s][5] = s_n[s][ty + 3][tx + 3];
+                qv[s][5] = s_vz[s][ty + 3][tx + 3];
+            }
         }
+        const int z = p - lag; // output plane
+        double fzhi[EX_QB];
+#pragma unroll
+        for (int s = 0; s < EX_QB; ++s) fzhi[s] = 0.0;
+        if (dim == 3 && P.do_transport && active && p >= zb + 2)
+        {
+#pragma unroll
+            for (int s = 0; s < EX_QB; ++s)
+            {
+                if (s >= nq) break;
+                double f = face_flux6(qn[s], qv[s], P.hyp_order, P.weno_scheme, dxmin, P.dt);
+                if (z == g.n[2] - 1 && wall_zero(P.bchi[q0 + s][2])) f = 0.0;
+                fzhi[s] = f;
+            }
+        }
+        if (z >= zb && active)
+        {
+            const long long t = g.idx(i, j, z);
+            double rx[EX_QB];
+            if (q0 == 0)
+            {
+                // reactions (update_rxnsrc_at_all_levels) for every component
+                double rxa[VD_NT];
+#pragma unroll
+                for (int c = 0; c < VD_NT; ++c) rxa[c] = 0.0;
+                if (P.do_reactions)
+                {
+                    double C[NUM_SPECIES], W[NUM_SPECIES];
+#pragma unroll
+                    for (int sp = 0; sp < NUM_SPECIES; sp++) C[sp] = S[sp * N + t] / N_A;
+                    double ee = 0.0;
+                    CKWC(P.Tg, C, W, S[ETEMP_ID * N + t], S[REF_ID * N + t], &ee);
+#pragma unroll
+                    for (int sp = 0; sp < NUM_SPECIES; sp++) rxa[sp] = W[sp] * N_A;
+                    rxa[NUM_SPECIES] = ee;
+#ifndef VD_NO_USER_REACT_SOURCES
+                    Array4 sv = state_view(const_cast<double*>(S), g);
+                    Array4 rv = cell_view(rxa, i, j, z);
+                    user_sources::add_user_react_sources(i, j, z, sv, rv, ga3(P.G.plo),
+                                                         ga3(P.G.phi), ga3(P.G.dx), P.time,
+                                                         *P.pp, P.Tg, P.Pg);
+#endif
+                }
+                if (P.rxn_een) P.rxn_een[t] = rxa[NUM_SPECIES];
+#pragma unroll
+                for (int sp = 0; sp < NUM_SPECIES; sp++)
+                    if (P.bg[sp]) P.expl[sp * N + t] = P.do_bg_rxn ? rxa[sp] : 0.0;
+                // reaction sources of components handled by later group launches
+                for (int q = EX_QB; q < P.ntr; ++q)
+                {
+                    const int comp = P.comp[q];
+#pragma unroll
+                    for (int c = 0; c < VD_NT; ++c)
+                        if (c == comp) P.expl[comp * N + t] = rxa[c];
+                }
+#pragma unroll
+                for (int s = 0; s < EX_QB; ++s)
+                {
+                    rx[s] = 0.0;
+                    if (s < nq)
+                    {
+                        const int comp = P.comp[s];
+#pragma unroll
+                        for (int c = 0; c < VD_NT; ++c)
+                            if (c == comp) rx[s] = rxa[c];
+                    }
+                }
+            } else
+            {
+#pragma unroll
+                for (int s = 0; s < EX_QB; ++s)
+                    rx[s] = (s < nq) ? P.expl[P.comp[q0 + s] * N + t] : 0.0;
+            }
+#pragma unroll
+            for (int s = 0; s < EX_QB; ++s)
+            {
+                if (s >= nq) break;
+                // divergences of plane z: three planes back in 3-D, this plane in 2-D
+                double v = ((dim == 3) ? qdx[s][0] : qdx[s][3]) + rx[s];
+                if (dim > 1) v += (dim == 3) ? qdy[s][0] : qdy[s][3];
+                if (dim == 3)
+                {
+                    double flo = fzlo[s];
+                    if (z == 0 && wall_zero(P.bclo[q0 + s][2])) flo = 0.0;
+                    v += (flo - fzhi[s]) / P.G.dx[2];
+                }
+                P.expl[P.comp[q0 + s] * N + t] = P.do_transport ? v : rx[s];
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < EX_QB; ++s) fzlo[s] = fzhi[s];
     }
 }
 
@@ -546,7 +732,9 @@ __device__ __forceinline__ double onesided_grad(const double* S, const GridDev& 
 
 __global__ void k_joule(JouleParams P)
 {
-    const GridDev& g = P.pot.op.g;
+    // the state is in natural layout; the Poisson level's grid may be red-black
+    GridDev g = P.pot.op.g;
+    g.rb = 0;
     const long long N = g.ncell();
     const double* __restrict__ S = P.S;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
@@ -713,8 +901,10 @@ __global__ void k_nonfinite(const double* __restrict__ S, long long n, unsigned 
 }
 
 template <typename T>
-__global__ void k_add_same(T* __restrict__ x, const T* __restrict__ e, long long n)
+__global__ void k_add_same(T* __restrict__ x, const T* __restrict__ e, long long n,
+                           const int* stop)
 {
+    if (stop && *(volatile const int*)stop) return;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x)
         x[t] += e[t];

@@ -16,6 +16,7 @@
 
 #include "vd_common.cuh"
 #include "vd_kernels.cuh"
+#include "vd_adjoint.cuh"
 
 #include <algorithm>
 #include <array>
@@ -268,7 +269,22 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
         for (int color = 0; color < 2; ++color)
         {
             if (prof) t_prof->begin(st);
-            if (op.g.rb)
+            T gamma = op.aconst; // interior diagonal of the constant-coefficient operator
+            for (int d = 0; d < op.g.dim; ++d) gamma += op.dh[d] * (op.bconst + op.bconst);
+            if (op.g.rb && op.g.dim == 3 && op.g.n[0] >= 4 && op.g.n[1] >= 4 &&
+                op.g.n[2] >= 4 && !op.a)
+            {
+                const int nxh = op.g.n[0] / 2;
+                const int bx = nxh >= 128 ? 128 : (nxh >= 64 ? 64 : (nxh >= 32 ? 32 : 16));
+                const int by = 256 / bx;
+                const dim3 grid((nxh + bx - 1) / bx, (op.g.n[1] + by - 1) / by, op.g.n[2]);
+                if (op.b[0])
+                    LAUNCH((k_mg_smooth_rb3<T, true>), grid, dim3(bx, by), st, op, x, f, color,
+                           inh ? 1 : 0, T(0));
+                else
+                    LAUNCH((k_mg_smooth_rb3<T, false>), grid, dim3(bx, by), st, op, x, f,
+                           color, inh ? 1 : 0, T(1) / gamma);
+            } else if (op.g.rb)
             {
                 const int nxh = op.g.n[0] / 2;
                 const int bx = nxh >= 128 ? 128 : (nxh >= 64 ? 64 : 32);
@@ -277,13 +293,8 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                     LAUNCH((k_mg_smooth_rb<T, true>), grid, bx, st, op, x, f, color,
                            inh ? 1 : 0, T(0));
                 else
-                {
-                    // interior diagonal of the constant-coefficient operator
-                    T gamma = op.aconst;
-                    for (int d = 0; d < op.g.dim; ++d) gamma += op.dh[d] * (op.bconst + op.bconst);
                     LAUNCH((k_mg_smooth_rb<T, false>), grid, bx, st, op, x, f, color,
                            inh ? 1 : 0, T(1) / gamma);
-                }
             } else
                 LAUNCH(k_mg_smooth_color<T>, gsz(half), BS, st, op, x, f, color, inh ? 1 : 0);
             if (prof) t_prof->end(st);
@@ -322,10 +333,14 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         LAUNCH(k_mg_resid_norm<T>, gn.g, gn.b, st, H.op[0], x0, f0, H.t0f, dscr, inh0 ? 1 : 0,
                0, 8);
         bottom(H, H.op[0], H.t0x, H.t0f, st);
-        LAUNCH(k_add_same<T>, gsz(H.g[0].ncell()), BS, st, x0, H.t0x, H.g[0].ncell());
+        LAUNCH(k_add_same<T>, gsz(H.g[0].ncell()), BS, st, x0, H.t0x, H.g[0].ncell(),
+               H.op[0].stop);
         return;
     }
-    for (int l = 0; l < L - 1; ++l)
+    // first level small enough for the one-CTA coarse cycle (never level 0)
+    int lc = L - 1;
+    while (lc > 1 && H.g[lc - 1].ncell() <= 4096) --lc;
+    for (int l = 0; l < lc; ++l)
     {
         T* xl = l ? H.x[l] : x0;
         T* fl = l ? H.f[l] : f0;
@@ -335,14 +350,36 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         LAUNCH(k_mg_resid_restrict<T>, gr.g, gr.b, st, H.op[l], xl, fl, H.g[l + 1], H.f[l + 1],
                H.x[l + 1], inh ? 1 : 0);
     }
-    bottom(H, H.op[L - 1], H.x[L - 1], H.f[L - 1], st);
-    for (int l = L - 2; l >= 0; --l)
+    if (lc == L - 1)
+        bottom(H, H.op[L - 1], H.x[L - 1], H.f[L - 1], st);
+    else
+    {
+        MGCoarse<T> C{};
+        C.lc = lc;
+        C.nl = L;
+        for (int l = lc; l < L; ++l)
+        {
+            C.op[l] = H.op[l];
+            C.x[l] = H.x[l];
+            C.f[l] = H.f[l];
+        }
+        // levels on chip when they fit (vd_create raises the kernel's dynamic
+        // shared-memory limit to VD_MG_COARSE_SMEM)
+        const size_t smem = mg_coarse_smem(C);
+        const int on_chip = smem <= VD_MG_COARSE_SMEM ? 1 : 0;
+        k_mg_coarse_vcycle<T><<<1, 512, on_chip ? smem : 0, st>>>(
+            C, H.scratch, T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf, on_chip);
+        ++vd::g_launches;
+        VD_CUDA_OK(cudaGetLastError());
+    }
+    for (int l = lc - 1; l >= 0; --l)
     {
         T* xl = l ? H.x[l] : x0;
         T* fl = l ? H.f[l] : f0;
         const bool inh = (l == 0) && inh0;
         const Grid3 gp = rows3(H.g[l]);
-        LAUNCH(k_mg_prolong_add<T>, gp.g, gp.b, st, H.g[l], H.g[l + 1], xl, H.x[l + 1]);
+        LAUNCH(k_mg_prolong_add<T>, gp.g, gp.b, st, H.g[l], H.g[l + 1], xl, H.x[l + 1],
+               H.op[l].stop);
         smooth(H.op[l], xl, fl, inh, H.nu2, st, l == 0 ? H.prof_tag : VD_PROF_NONE);
     }
 }
@@ -374,6 +411,11 @@ struct Ctx
     ProbParm* dpp = nullptr;
     unsigned long long* dscal = nullptr;
     unsigned long long* hscal = nullptr;
+    double* dpart = nullptr; // per-block partial maxima of the residual norm
+    long long npart = 0;
+    MGDev* dmg = nullptr;   // device-side solve state (asynchronous V-cycles)
+    MGDev* hmg = nullptr;   // pinned host mirror
+    int hint[VD_NT + 1] = {}; // last V-cycle count per solve (index VD_NT: Poisson)
     double time = 0.0;
     int step = 0;
     int eidx = E_ID;
@@ -386,6 +428,7 @@ struct Ctx
     long long poisson_iters = 0, species_iters = 0;
     int not_converged = 0;
     double max_poisson_res = 0.0;
+    struct AdjState* adjs = nullptr; // discrete-adjoint buffers, made on first use
 };
 
 std::string g_create_err;
@@ -457,14 +500,39 @@ double read_norm(Ctx& c)
     return v;
 }
 
+// Residual max-norm in two stages (per-block maxima, then one block), into
+// the bit patterns at mx[0] (|r|) and mx[1] (|f| when `fnorm`).
+template <typename T>
+void launch_norm(Ctx& c, const MGOp<T>& op, const T* x, const T* f, T* rout, bool inh,
+                 bool fnorm, unsigned long long* mx)
+{
+    if (op.g.rb)
+    {
+        const long long half = op.g.ncell() >> 1;
+        const long long nb = std::min<long long>((half + 255) / 256, c.npart);
+        LAUNCH(k_mg_resid_norm_rb<T>, dim3((unsigned)nb), 256, c.st, op, x, f, rout,
+               inh ? 1 : 0, fnorm ? 1 : 0, c.dpart);
+        LAUNCH(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nb, fnorm ? 1 : 0, mx);
+        return;
+    }
+    int rows = 8;
+    Grid3 gn = rows3(op.g, rows);
+    while ((long long)gn.g.x * gn.g.y * gn.g.z > c.npart)
+    {
+        rows *= 2;
+        gn = rows3(op.g, rows);
+    }
+    const long long nb = (long long)gn.g.x * gn.g.y * gn.g.z;
+    LAUNCH(k_mg_resid_norm<T>, gn.g, gn.b, c.st, op, x, f, rout, mx, inh ? 1 : 0,
+           fnorm ? 1 : 0, rows, c.dpart);
+    LAUNCH(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nb, fnorm ? 1 : 0, mx);
+}
+
 template <typename T>
 double resid_norm(Ctx& c, const MGOp<T>& op, const T* x, const T* f, T* rout, bool inh,
                   double* fnorm = nullptr)
 {
-    VD_CUDA_OK(cudaMemsetAsync(c.dscal, 0, 2 * sizeof(unsigned long long), c.st));
-    const Grid3 gn = rows3(op.g, 8);
-    LAUNCH(k_mg_resid_norm<T>, gn.g, gn.b, c.st, op, x, f, rout, c.dscal, inh ? 1 : 0,
-           fnorm ? 1 : 0, 8);
+    launch_norm(c, op, x, f, rout, inh, fnorm != nullptr, c.dscal);
     if (fnorm)
     {
         VD_CUDA_OK(cudaMemcpyAsync(c.hscal + 1, c.dscal + 1, sizeof(unsigned long long),
@@ -523,7 +591,7 @@ void bind_sides32(Ctx& c, Hier<float>& H, SideArrays* sides, const int* bct)
 // solution.  Refined: FP64 residual, FP32 V-cycles on the normalised
 // correction, FP64 update; both stop on |r|_inf <= max(abs, rel |r0|_inf).
 int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* rhs,
-             vd_solve_stats* stats)
+             vd_solve_stats* stats, int hint = 1)
 {
     const vd_config& cfg = c.cfg;
     double b0 = 0.0;
@@ -567,18 +635,34 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
             }
         } else
         {
-            for (int it = 1; it <= cfg.linsolve_maxiter; ++it)
+            // V-cycles are enqueued in batches; each kernel returns at once
+            // when the device-side stop flag is up, so the iteration count
+            // and result equal those of a cycle-by-cycle host loop
+            VD_CUDA_OK(cudaMemsetAsync(c.dmg, 0, sizeof(MGDev), c.st));
+            for (auto& o : H64.op) o.stop = &c.dmg->done;
+            MGOp<double> op0 = H64.op[0];
+            int issued = 0;
+            int batch = std::max(1, hint - 1);
+            while (issued < cfg.linsolve_maxiter)
             {
-                vcycle(H64, sol, rhs, true, c.dscal, c.st);
-                st.iterations = it;
-                const double rn = resid_norm(c, H64.op[0], sol, rhs, (double*)nullptr, true);
-                st.final_residual = rn;
-                if (rn <= target)
+                const int nb = std::min(batch, cfg.linsolve_maxiter - issued);
+                for (int b = 0; b < nb; ++b)
                 {
-                    st.converged = 1;
-                    break;
+                    vcycle(H64, sol, rhs, true, c.dscal, c.st);
+                    launch_norm(c, op0, (const double*)sol, (const double*)rhs, (double*)nullptr,
+                                true, false, &c.dmg->rbits);
+                    LAUNCH(k_mg_check, 1, 1, c.st, c.dmg, target);
+                    ++issued;
                 }
+                VD_CUDA_OK(cudaMemcpyAsync(c.hmg, c.dmg, sizeof(MGDev), cudaMemcpyDeviceToHost, c.st));
+                VD_CUDA_OK(cudaStreamSynchronize(c.st));
+                if (c.hmg->done) break;
+                batch = 2;
             }
+            for (auto& o : H64.op) o.stop = nullptr;
+            st.iterations = c.hmg->iters;
+            std::memcpy(&st.final_residual, &c.hmg->final_bits, sizeof(double));
+            st.converged = c.hmg->done;
         }
     }
     if (stats) *stats = st;
@@ -616,11 +700,15 @@ void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats)
             LAUNCH(k_inneu_adjust, gsz(plane_count(c.g, s % 3)), BS, c.st, c.HP.g[0], s,
                    (const double*)nullptr, -1.0, 1.0, c.G.dx[s % 3], c.pside[s].val, c.phi_rhs);
     vd_solve_stats st{};
-    const int it = mg_solve(c, c.HP, c.HP32, c.phi_sol, c.phi_rhs, &st);
+    const int it = mg_solve(c, c.HP, c.HP32, c.phi_sol, c.phi_rhs, &st, c.hint[VD_NT]);
+    if (st.converged && it > 0) c.hint[VD_NT] = it;
     c.poisson_iters += it;
     c.max_poisson_res = std::max(c.max_poisson_res, st.final_residual);
     if (stats) *stats = st;
-    LAUNCH(k_efield, gsz(c.N), BS, c.st, grad_ctx(c, c.HP, c.pside), c.phi_sol, c.S, ps);
+    {
+        const Grid3 ge = rows3(c.g);
+        LAUNCH(k_efield, ge.g, ge.b, c.st, grad_ctx(c, c.HP, c.pside), c.phi_sol, c.S, ps);
+    }
 }
 
 // ---- explicit sources of every transported component
@@ -680,7 +768,12 @@ void explicit_rhs(Ctx& c, double time)
         t_prof->bytes = 8.0 * (nin + nout) * (double)c.N;
         t_prof->begin(c.st);
     }
-    LAUNCH(k_explicit, gsz(c.N), BS, c.st, P);
+    // streaming kernel: one launch per group of EX_QB components
+    const int zc = (cfg.dim == 3) ? std::min(32, c.g.n[2]) : 1;
+    const dim3 grid((c.g.n[0] + EX_TX - 1) / EX_TX, (c.g.n[1] + EX_TY - 1) / EX_TY,
+                    (c.g.n[2] + zc - 1) / zc);
+    for (int q0 = 0; q0 < std::max(n, 1); q0 += EX_QB)
+        LAUNCH(k_explicit_stream, grid, EX_TX * EX_TY, c.st, P, q0, zc);
     if (prof) t_prof->end(c.st);
 }
 
@@ -717,7 +810,8 @@ void species_solve(Ctx& c, int comp, double time, const double* Sold, vd_solve_s
                    (const double*)c.HS.bf[0][s % 3], 1.0, ts, c.G.dx[s % 3], c.sside[s].val,
                    c.spec_rhs);
     vd_solve_stats st{};
-    const int it = mg_solve(c, c.HS, c.HS32, c.u[comp], c.spec_rhs, &st);
+    const int it = mg_solve(c, c.HS, c.HS32, c.u[comp], c.spec_rhs, &st, c.hint[comp]);
+    if (st.converged && it > 0) c.hint[comp] = it;
     c.species_iters += it;
     if (stats) *stats = st;
 }
@@ -886,6 +980,201 @@ const Key g_keys[] = {
     KI("vidyut.mg_inner_cycles", mg_inner_cycles),
     KI("vidyut.poisson_warm_start", poisson_warm_start), KI("vidyut.device", device),
 };
+
+
+// ---- discrete adjoint of N explicit flux + source steps (vd_adjoint.cuh)
+struct AdjState
+{
+    Alloc A;
+    int nt = 0;                 // transported species
+    int spec[NUM_SPECIES] = {}; // their components, ascending
+    int eslot = -1;
+    std::vector<double*> slot;  // state slots, nt x N each
+    double* mu = nullptr;
+    double* dmu = nullptr;
+    double* lam = nullptr;
+    double* adj = nullptr;
+    double* adjnd = nullptr;
+    double* theta = nullptr; // device log pre-factor shifts
+    double* acc = nullptr;   // [0] J, [1..R] dJ/dtheta_r, [R+1] dJ/dscale
+    double* hacc = nullptr;  // pinned mirror of acc
+    std::vector<double> params; // theta_0 .. theta_{R-1}, electron mobility scale
+    ~AdjState()
+    {
+        A.release();
+        if (hacc) cudaFreeHost(hacc);
+    }
+};
+
+#ifdef VD_HAS_MECH_ADJOINT
+constexpr int ADJ_NR = NUM_REACTIONS;
+
+dim3 gsz128(long long n)
+{
+    long long b = (n + 127) / 128;
+    if (b < 1) b = 1;
+    if (b > 148LL * 64) b = 148LL * 64;
+    return dim3((unsigned)b);
+}
+
+AdjState& adj_state(Ctx& c, int slots)
+{
+    const long long N = c.N;
+    if (!c.adjs)
+    {
+        AdjState* a = new AdjState();
+        c.adjs = a;
+        for (int sp = 0; sp < NUM_SPECIES; ++sp)
+            if (!c.bg[sp])
+            {
+                if (sp == c.eidx) a->eslot = a->nt;
+                a->spec[a->nt++] = sp;
+            }
+        if (a->eslot < 0) throw CudaError("the electrons are a background species");
+        a->mu = a->A.get<double>((size_t)a->nt * N);
+        a->dmu = a->A.get<double>((size_t)a->nt * N);
+        a->lam = a->A.get<double>((size_t)a->nt * N);
+        a->adj = a->A.get<double>((size_t)a->nt * N);
+        a->adjnd = a->A.get<double>(N);
+        a->theta = a->A.get<double>(ADJ_NR);
+        a->acc = a->A.get<double>(ADJ_NR + 2);
+        VD_CUDA_OK(cudaMallocHost(&a->hacc, sizeof(double) * (ADJ_NR + 2)));
+        a->params.assign(ADJ_NR + 1, 0.0);
+        a->params[ADJ_NR] = 1.0;
+    }
+    AdjState& a = *c.adjs;
+    while ((int)a.slot.size() < slots) a.slot.push_back(a.A.get<double>((size_t)a.nt * N));
+    return a;
+}
+
+AdjParams adj_params(Ctx& c, AdjState& a)
+{
+    AdjParams P{};
+    P.g = c.g;
+    P.g.rb = 0;
+    for (int d = 0; d < 3; ++d) P.dx[d] = c.G.dx[d];
+    P.dt = c.cfg.dt;
+    P.dxmin = c.G.dx[0];
+    for (int d = 1; d < c.cfg.dim; ++d) P.dxmin = std::min(P.dxmin, c.G.dx[d]);
+    P.Tg = c.cfg.gas_temperature;
+    P.mob_scale = a.params[ADJ_NR];
+    P.hyp_order = c.cfg.hyp_order;
+    P.weno_scheme = c.cfg.weno_scheme;
+    P.nt = a.nt;
+    P.eslot = a.eslot;
+    for (int s = 0; s < a.nt; ++s)
+    {
+        P.spec[s] = a.spec[s];
+        for (int d = 0; d < 3; ++d)
+        {
+            P.bclo[s][d] = bclo_for(c, a.spec[s])[d];
+            P.bchi[s][d] = bchi_for(c, a.spec[s])[d];
+        }
+    }
+    P.S = c.S;
+    P.theta = a.theta;
+    P.mu = a.mu;
+    P.dmu = a.dmu;
+    return P;
+}
+
+void adj_step(Ctx& c, const AdjParams& P, const double* from, double* to)
+{
+    LAUNCH(k_adj_props, gsz(c.N), BS, c.st, P, from);
+    LAUNCH(k_adj_step, gsz(c.N), BS, c.st, P, from, to);
+}
+
+double adj_cell_volume(const Ctx& c)
+{
+    double dv = 1.0;
+    for (int d = 0; d < c.cfg.dim; ++d) dv *= c.G.dx[d];
+    return dv;
+}
+
+// Forward sweep from the state's transported species.  With K > 0 the state
+// at every step k = bK is kept in slot b; the objective is added into acc[0].
+// Returns the slot holding the final state.
+double* adj_forward(Ctx& c, AdjState& a, const AdjParams& P, int nsteps, int K)
+{
+    const long long N = c.N;
+    const int nck = (K > 0) ? (nsteps + K - 1) / K : 1;
+    double* w[2] = {a.slot[nck], a.slot[nck + 1]};
+    double* cur = a.slot[0];
+    for (int s = 0; s < a.nt; ++s)
+        VD_CUDA_OK(cudaMemcpyAsync(cur + (size_t)s * N, c.S + (size_t)a.spec[s] * N,
+                                   sizeof(double) * N, cudaMemcpyDeviceToDevice, c.st));
+    for (int k = 0; k < nsteps; ++k)
+    {
+        double* nxt;
+        if (K > 0 && (k + 1) % K == 0 && k + 1 < nsteps)
+            nxt = a.slot[(k + 1) / K];
+        else
+            nxt = (cur == w[0]) ? w[1] : w[0];
+        adj_step(c, P, cur, nxt);
+        cur = nxt;
+    }
+    LAUNCH(k_adj_objective, gsz(N), BS, c.st, N, cur + (size_t)a.eslot * N,
+           adj_cell_volume(c), a.acc);
+    return cur;
+}
+
+void adj_read_acc(Ctx& c, AdjState& a)
+{
+    VD_CUDA_OK(cudaMemcpyAsync(a.hacc, a.acc, sizeof(double) * (ADJ_NR + 2),
+                               cudaMemcpyDeviceToHost, c.st));
+    VD_CUDA_OK(cudaStreamSynchronize(c.st));
+}
+
+void adj_upload(Ctx& c, AdjState& a)
+{
+    VD_CUDA_OK(cudaMemcpyAsync(a.theta, a.params.data(), sizeof(double) * ADJ_NR,
+                               cudaMemcpyHostToDevice, c.st));
+    VD_CUDA_OK(cudaMemsetAsync(a.acc, 0, sizeof(double) * (ADJ_NR + 2), c.st));
+}
+
+// Gradient of the objective by the backward sweep: checkpoints every K steps,
+// the states of each K-block recomputed from its checkpoint.
+void adj_run(Ctx& c, int nsteps, int K)
+{
+    const long long N = c.N;
+    const int nck = (nsteps + K - 1) / K;
+    const int ntraj = std::max(K, 2);
+    AdjState& a = adj_state(c, nck + ntraj);
+    const AdjParams P = adj_params(c, a);
+    adj_upload(c, a);
+    adj_forward(c, a, P, nsteps, K);
+    // lambda = dJ/du at the last step: dV on the electrons
+    VD_CUDA_OK(cudaMemsetAsync(a.lam, 0, sizeof(double) * (size_t)a.nt * N, c.st));
+    LAUNCH(k_fill<double>, gsz(N), BS, c.st, a.lam + (size_t)a.eslot * N, adj_cell_volume(c), N);
+    std::vector<double*> t(ntraj);
+    for (int b = nck - 1; b >= 0; --b)
+    {
+        const int k0 = b * K, k1 = std::min(nsteps, k0 + K);
+        t[0] = a.slot[b];
+        for (int i = 1; i < k1 - k0; ++i)
+        {
+            t[i] = a.slot[nck + i];
+            adj_step(c, P, t[i - 1], t[i]);
+        }
+        for (int k = k1 - 1; k >= k0; --k)
+        {
+            const double* uk = t[k - k0];
+            LAUNCH(k_adj_props, gsz(N), BS, c.st, P, uk);
+            VD_CUDA_OK(cudaMemsetAsync(a.adj, 0, sizeof(double) * (size_t)a.nt * N, c.st));
+            VD_CUDA_OK(cudaMemsetAsync(a.adjnd, 0, sizeof(double) * N, c.st));
+            for (int d = 0; d < c.cfg.dim; ++d)
+            {
+                const long long nf = N / c.g.n[d] * (c.g.n[d] + 1);
+                LAUNCH(k_adj_faces, gsz128(nf), 128, c.st, P, d, uk, a.lam, a.adj, a.adjnd,
+                       a.acc + 1 + ADJ_NR);
+            }
+            LAUNCH(k_adj_chem_update, gsz128(N), 128, c.st, P, uk, a.lam, a.adj, a.adjnd,
+                   a.acc + 1);
+        }
+    }
+    adj_read_acc(c, a);
+}
+#endif // VD_HAS_MECH_ADJOINT
 
 } // namespace
 
@@ -1123,6 +1412,12 @@ vd_status vd_create(const vd_config* cfg, void** out)
             h->nu1 = cfg->linsolve_num_pre_smooth;
             h->nu2 = cfg->linsolve_num_post_smooth;
         }
+        VD_CUDA_OK(cudaFuncSetAttribute(k_mg_coarse_vcycle<double>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        VD_MG_COARSE_SMEM));
+        VD_CUDA_OK(cudaFuncSetAttribute(k_mg_coarse_vcycle<float>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        VD_MG_COARSE_SMEM));
         c->HP.prof_tag = VD_PROF_POISSON_SMOOTH;
         c->HP32.prof_tag = VD_PROF_POISSON_SMOOTH32;
         VD_CUDA_OK(cudaEventCreate(&c->ev0));
@@ -1131,6 +1426,10 @@ vd_status vd_create(const vd_config* cfg, void** out)
         VD_CUDA_OK(cudaMemcpy(c->dpp, &c->hpp, sizeof(ProbParm), cudaMemcpyHostToDevice));
         c->dscal = c->A.get<unsigned long long>(2);
         VD_CUDA_OK(cudaMallocHost(&c->hscal, 2 * sizeof(unsigned long long)));
+        c->dmg = c->A.get<MGDev>(1);
+        c->npart = 65536;
+        c->dpart = c->A.get<double>(2 * c->npart);
+        VD_CUDA_OK(cudaMallocHost(&c->hmg, sizeof(MGDev)));
         // electron index (Source/Vidyut.cpp:132-144)
         c->eidx = E_ID;
         VD_CUDA_OK(cudaDeviceSynchronize());
@@ -1157,6 +1456,8 @@ vd_status vd_destroy(void* ctx)
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->hscal) cudaFreeHost(c->hscal);
+    if (c->hmg) cudaFreeHost(c->hmg);
+    delete c->adjs;
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
     return VD_OK;
@@ -1346,6 +1647,85 @@ vd_status vd_check_state(void* ctx, long long* nonfinite)
     return *nonfinite ? VD_ERR_NONFINITE : VD_OK;
 }
 
+vd_status vd_adjoint_num_params(void* ctx, int* n_params)
+{
+    if (!ctx || !n_params) return VD_ERR_INVALID_ARG;
+#ifdef VD_HAS_MECH_ADJOINT
+    *n_params = ADJ_NR + 1;
+#else
+    *n_params = 0;
+#endif
+    return VD_OK;
+}
+
+#ifdef VD_HAS_MECH_ADJOINT
+#define VD_ADJ_CASE_CHECK
+#else
+#define VD_ADJ_CASE_CHECK                                                        \
+    {                                                                            \
+        static_cast<Ctx*>(ctx)->err = "this case's mechanism has no adjoint form"; \
+        return VD_ERR_UNSUPPORTED;                                               \
+    }
+#endif
+
+vd_status vd_adjoint_set_params(void* ctx, const double* params, int n_params)
+{
+    if (!ctx || !params) return VD_ERR_INVALID_ARG;
+    VD_ADJ_CASE_CHECK
+#ifdef VD_HAS_MECH_ADJOINT
+    if (n_params != ADJ_NR + 1 || !(params[ADJ_NR] > 0.0))
+    {
+        static_cast<Ctx*>(ctx)->err = "expected NUM_REACTIONS log pre-factor shifts and a "
+                                      "positive electron mobility scale";
+        return VD_ERR_INVALID_ARG;
+    }
+    VD_TRY({
+        AdjState& a = adj_state(*c, 0);
+        a.params.assign(params, params + ADJ_NR + 1);
+    });
+#endif
+    return VD_OK;
+}
+
+vd_status vd_adjoint_forward(void* ctx, int nsteps, int objective_id, double* objective,
+                             double* species_out)
+{
+    if (!ctx || nsteps < 0 || objective_id != VD_ADJ_OBJ_ELECTRONS) return VD_ERR_INVALID_ARG;
+    VD_ADJ_CASE_CHECK
+#ifdef VD_HAS_MECH_ADJOINT
+    VD_TRY({
+        AdjState& a = adj_state(*c, 3);
+        const AdjParams P = adj_params(*c, a);
+        adj_upload(*c, a);
+        const double* fin = adj_forward(*c, a, P, nsteps, 0);
+        if (species_out)
+            VD_CUDA_OK(cudaMemcpyAsync(species_out, fin, sizeof(double) * (size_t)a.nt * c->N,
+                                       cudaMemcpyDeviceToHost, c->st));
+        adj_read_acc(*c, a);
+        if (objective) *objective = a.hacc[0];
+    });
+#endif
+    return VD_OK;
+}
+
+vd_status vd_adjoint_run(void* ctx, int nsteps, int K, int objective_id, double* objective,
+                         double* grad_out, int n_params)
+{
+    if (!ctx || nsteps < 1 || K < 1 || objective_id != VD_ADJ_OBJ_ELECTRONS || !grad_out)
+        return VD_ERR_INVALID_ARG;
+    VD_ADJ_CASE_CHECK
+#ifdef VD_HAS_MECH_ADJOINT
+    if (n_params != ADJ_NR + 1) return VD_ERR_INVALID_ARG;
+    VD_TRY({
+        adj_run(*c, nsteps, K);
+        AdjState& a = *c->adjs;
+        if (objective) *objective = a.hacc[0];
+        for (int r = 0; r <= ADJ_NR; ++r) grad_out[r] = a.hacc[1 + r];
+    });
+#endif
+    return VD_OK;
+}
+
 vd_status vd_launch_count(void* ctx, long long* launches)
 {
     if (!launches) return VD_ERR_INVALID_ARG;
@@ -1439,7 +1819,8 @@ int na_vcycle(NAHier& H, double* x0, const double* f0, char* err, int errlen)
                   0, 8);
         NA_LAUNCH(k_mg_bottom<double>, 1, 256, H.op[0], H.t0x, H.t0f, H.scratch, 1e-4, 200, 0,
                   8, (int*)nullptr);
-        NA_LAUNCH(k_add_same<double>, gsz(H.g[0].ncell()), BS, x0, H.t0x, H.g[0].ncell());
+        NA_LAUNCH(k_add_same<double>, gsz(H.g[0].ncell()), BS, x0, H.t0x, H.g[0].ncell(),
+                  (const int*)nullptr);
         return VD_OK;
     }
     for (int l = 0; l < L; ++l)
@@ -1466,7 +1847,8 @@ int na_vcycle(NAHier& H, double* x0, const double* f0, char* err, int errlen)
         double* xl = l ? H.x[l] : x0;
         const double* fl = l ? H.f[l] : f0;
         const Grid3 gp = rows3(H.g[l]);
-        NA_LAUNCH(k_mg_prolong_add<double>, gp.g, gp.b, H.g[l], H.g[l + 1], xl, H.x[l + 1]);
+        NA_LAUNCH(k_mg_prolong_add<double>, gp.g, gp.b, H.g[l], H.g[l + 1], xl, H.x[l + 1],
+                  (const int*)nullptr);
         for (int s = 0; s < 2; ++s)
             for (int color = 0; color < 2; ++color)
                 NA_LAUNCH(k_mg_smooth_color<double>,

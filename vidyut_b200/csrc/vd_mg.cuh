@@ -46,7 +46,14 @@ struct MGOp
     T c1s[6];
     const T* c0[6];
     const T* gv[6];
+    const int* stop; // set to non-zero on the device once the solve has converged
 };
+
+template <typename T>
+__device__ __forceinline__ bool mg_stopped(const MGOp<T>& L)
+{
+    return L.stop && *(volatile const int*)L.stop;
+}
 
 __host__ __device__ inline int plane_index(const GridDev& g, int d, int i, int j, int k)
 {
@@ -197,6 +204,7 @@ template <typename T>
 __global__ void k_mg_smooth_color(MGOp<T> L, T* __restrict__ x,
                                   const T* __restrict__ f, int color, int inhomog)
 {
+    if (mg_stopped(L)) return;
     const int nxh = (L.g.n[0] + 1) >> 1;
     const long long tot = (long long)nxh * L.g.n[1] * L.g.n[2];
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
@@ -222,6 +230,7 @@ __global__ void __launch_bounds__(128) k_mg_smooth_rb(MGOp<T> L, T* __restrict__
                                                       const T* __restrict__ f, int color,
                                                       int inhomog, T inv_gamma)
 {
+    if (mg_stopped(L)) return;
     const GridDev& g = L.g;
     const int nxh = g.n[0] >> 1;
     const int ih = blockIdx.x * blockDim.x + threadIdx.x;
@@ -275,6 +284,96 @@ __global__ void __launch_bounds__(128) k_mg_smooth_rb(MGOp<T> L, T* __restrict__
         // x0 + (f - (gamma x0 - rho)) / gamma = (f + rho) / gamma
         xs[h] = (fv + rho) * inv_gamma;
     }
+}
+
+// One Gauss-Seidel colour on a 3-D red-black split level (nx, ny, nz >= 4),
+// one cell per thread on a (half-row x rows x planes) grid.  Rows with j or
+// k on the boundary take the general path (whole warps, no divergence);
+// in every other row the two x-boundary cells are folded into the fast
+// path: the ghost value c0 x0 + c1 x1 + g of the boundary side contributes
+// c1 x1 + g to the neighbour sum and c0 to the diagonal, which is the same
+// cell equation mg_gs_cell solves (x0 cancels out of the exact update), and
+// periodic x wraps to the row's other end.
+template <typename T, bool VARB>
+__global__ void __launch_bounds__(256) k_mg_smooth_rb3(MGOp<T> L, T* __restrict__ x,
+                                                       const T* __restrict__ f, int color,
+                                                       int inhomog, T inv_gamma)
+{
+    if (mg_stopped(L)) return;
+    const GridDev& g = L.g;
+    const int nx = g.n[0], nxh = nx >> 1, ny = g.n[1], nz = g.n[2];
+    const int ih = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (ih >= nxh || j >= ny) return;
+    const int q = (j + k + color) & 1;
+    const int i = 2 * ih + q;
+    if (j == 0 || j == ny - 1 || k == 0 || k == nz - 1)
+    {
+        mg_gs_cell(L, x, f, i, j, k, inhomog != 0);
+        return;
+    }
+    const long long half = g.ncell() >> 1;
+    const long long plane = (long long)nxh * ny;
+    const long long r = j + (long long)ny * k;
+    const long long row = (long long)nxh * r;
+    const long long h = ih + row;
+    T* __restrict__ xs = x + color * half;
+    const T* __restrict__ xo = x + (1 - color) * half;
+    const bool lo = (i == 0), hi = (i == nx - 1);
+    // x neighbours in the other colour: h-1+q and h+q, wrapped or replaced at the ends
+    long long im = h - 1 + q, ip = h + q;
+    if (lo) im = g.per[0] ? row + nxh - 1 : ip;
+    if (hi) ip = g.per[0] ? row : im;
+    T xm = xo[im], xp = xo[ip];
+    const T ym = xo[h - nxh], yp = xo[h + nxh];
+    const T zm = xo[h - plane], zp = xo[h + plane];
+    const T fv = f[color * half + h];
+    const T dhx = L.dh[0], dhy = L.dh[1], dhz = L.dh[2];
+    T bxl, bxh, byl, byh, bzl, bzh;
+    if (VARB)
+    {
+        const long long fx = i + (long long)(nx + 1) * r;
+        bxl = L.b[0][fx];
+        bxh = L.b[0][fx + 1];
+        const long long fy = i + (long long)nx * (j + (long long)(ny + 1) * k);
+        byl = L.b[1][fy];
+        byh = L.b[1][fy + nx];
+        const long long fz = i + (long long)nx * r;
+        bzl = L.b[2][fz];
+        bzh = L.b[2][fz + (long long)nx * ny];
+    } else
+        bxl = bxh = byl = byh = bzl = bzh = L.bconst;
+    T dsub = T(0); // boundary coefficient absorbed into the diagonal
+    if ((lo || hi) && !g.per[0])
+    {
+        const int s = lo ? 0 : 3;
+        const int p = j + ny * k;
+        const T c0 = L.c0[s] ? L.c0[s][p] : L.c0s[s];
+        T gh = L.c1s[s] * (lo ? xp : xm);
+        if (inhomog && L.gv[s]) gh += L.gv[s][p];
+        if (lo)
+        {
+            xm = gh;
+            dsub = dhx * bxl * c0;
+        } else
+        {
+            xp = gh;
+            dsub = dhx * bxh * c0;
+        }
+    }
+    T rho = dhx * (bxl * xm + bxh * xp);
+    rho += dhy * (byl * ym + byh * yp);
+    rho += dhz * (bzl * zm + bzh * zp);
+    if (VARB || dsub != T(0))
+    {
+        T gamma = L.aconst;
+        gamma += dhx * (bxl + bxh);
+        gamma += dhy * (byl + byh);
+        gamma += dhz * (bzl + bzh);
+        xs[h] = (fv + rho) / (gamma - dsub);
+    } else
+        xs[h] = (fv + rho) * inv_gamma;
 }
 
 // L(x) at an interior cell of a red-black split level, neighbours addressed
@@ -342,6 +441,7 @@ __global__ void __launch_bounds__(128) k_mg_resid_restrict(MGOp<T> L, const T* _
                                                            T* __restrict__ fc,
                                                            T* __restrict__ xc, int inhomog)
 {
+    if (mg_stopped(L)) return;
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= gc.n[0]) return;
     const int J = blockIdx.y, K = blockIdx.z;
@@ -363,18 +463,23 @@ __global__ void __launch_bounds__(128) k_mg_resid_restrict(MGOp<T> L, const T* _
 // Max-norm of f - L(x) into mx[0] (and of f into mx[1] when `fnorm`); the
 // residual itself into rout when given.  Grid: (row blocks, ny/rows, nz),
 // each thread walking `rows` rows.
+// With `part` given, each block stores its maxima in part[b] (and
+// part[nblocks + b] for |f|) for k_mg_max_partials instead of using atomics.
 template <typename T>
 __global__ void __launch_bounds__(128) k_mg_resid_norm(MGOp<T> L, const T* __restrict__ x,
                                                        const T* __restrict__ f,
                                                        T* __restrict__ rout,
                                                        unsigned long long* mx, int inhomog,
-                                                       int fnorm, int rows)
+                                                       int fnorm, int rows,
+                                                       double* part = nullptr)
 {
+    if (mg_stopped(L)) return;
     __shared__ double sh[32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.z;
     double m = 0.0, mf = 0.0;
     if (i < L.g.n[0])
+#pragma unroll 4
         for (int jj = 0; jj < rows; ++jj)
         {
             const int j = blockIdx.y * rows + jj;
@@ -391,19 +496,102 @@ __global__ void __launch_bounds__(128) k_mg_resid_norm(MGOp<T> L, const T* __res
             }
         }
     m = block_max(m, sh);
-    if (threadIdx.x == 0) atomic_max_nonneg(mx, m);
-    if (fnorm)
+    if (fnorm) mf = block_max(mf, sh);
+    if (threadIdx.x == 0)
     {
-        mf = block_max(mf, sh);
-        if (threadIdx.x == 0) atomic_max_nonneg(mx + 1, mf);
+        if (part)
+        {
+            const long long nb = (long long)gridDim.x * gridDim.y * gridDim.z;
+            const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+            part[b] = m;
+            if (fnorm) part[nb + b] = mf;
+        } else
+        {
+            atomic_max_nonneg(mx, m);
+            if (fnorm) atomic_max_nonneg(mx + 1, mf);
+        }
+    }
+}
+
+// Residual max-norm on a red-black split level: one thread per half-row
+// position h = (i/2, j, k), i.e. per pair of cells 2(i/2) and 2(i/2)+1 (one
+// of each colour, both at offset h of their colour half), grid-stride over
+// the pairs.  Per-block maxima go to part[b] (and part[gridDim.x + b] for
+// |f|) for k_mg_max_partials; the residual itself to rout when given.
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_resid_norm_rb(MGOp<T> L, const T* __restrict__ x,
+                                                          const T* __restrict__ f,
+                                                          T* __restrict__ rout, int inhomog,
+                                                          int fnorm, double* __restrict__ part)
+{
+    if (mg_stopped(L)) return;
+    __shared__ double sh[32];
+    const GridDev& g = L.g;
+    const int nxh = g.n[0] >> 1, ny = g.n[1];
+    const long long half = g.ncell() >> 1;
+    double m = 0.0, mf = 0.0;
+    for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < half;
+         h += (long long)gridDim.x * blockDim.x)
+    {
+        const int ih = (int)(h % nxh);
+        const long long r = h / nxh;
+        const int j = (int)(r % ny), k = (int)(r / ny);
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+        {
+            const int i = 2 * ih + s;
+            const long long p = (long long)((i + j + k) & 1) * half + h;
+            const T rr = f[p] - mg_apply_any(L, x, i, j, k, inhomog != 0);
+            if (rout) rout[p] = rr;
+            const double a = fabs((double)rr);
+            m = a > m ? a : m;
+            if (fnorm)
+            {
+                const double af = fabs((double)f[p]);
+                mf = af > mf ? af : mf;
+            }
+        }
+    }
+    m = block_max(m, sh);
+    if (fnorm) mf = block_max(mf, sh);
+    if (threadIdx.x == 0)
+    {
+        part[blockIdx.x] = m;
+        if (fnorm) part[gridDim.x + blockIdx.x] = mf;
+    }
+}
+
+// Second stage of the residual max-norm: one block reduces the per-block
+// partial maxima and stores the bit patterns in mx[0] (and mx[1]).
+template <typename T>
+__global__ void __launch_bounds__(1024) k_mg_max_partials(MGOp<T> L, const double* part,
+                                                          long long nb, int fnorm,
+                                                          unsigned long long* mx)
+{
+    if (mg_stopped(L)) return;
+    __shared__ double sh[32];
+    double m = 0.0, mf = 0.0;
+    for (long long b = threadIdx.x; b < nb; b += blockDim.x)
+    {
+        m = part[b] > m ? part[b] : m;
+        if (fnorm) mf = part[nb + b] > mf ? part[nb + b] : mf;
+    }
+    m = block_max(m, sh);
+    if (fnorm) mf = block_max(mf, sh);
+    if (threadIdx.x == 0)
+    {
+        mx[0] = (unsigned long long)__double_as_longlong(m);
+        if (fnorm) mx[1] = (unsigned long long)__double_as_longlong(mf);
     }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(128) k_mg_prolong_add(GridDev gf, GridDev gc,
                                                         T* __restrict__ xf,
-                                                        const T* __restrict__ xc)
+                                                        const T* __restrict__ xc,
+                                                        const int* stop)
 {
+    if (stop && *(volatile const int*)stop) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= gf.n[0]) return;
     const int j = blockIdx.y, k = blockIdx.z;
@@ -416,11 +604,10 @@ __global__ void __launch_bounds__(128) k_mg_prolong_add(GridDev gf, GridDev gc,
 // Gauss-Seidel smooths (or `nuf` when BiCGStab did not converge).  Every
 // vector is addressed through the level's layout (L.g.idx), like x and b.
 template <typename T>
-__global__ void k_mg_bottom(MGOp<T> L, T* __restrict__ x, const T* __restrict__ b,
-                            T* __restrict__ scr, T rel, int maxiter, int nub, int nuf,
-                            int* status)
+__device__ void mg_bottom_block(const MGOp<T>& L, T* __restrict__ x, const T* __restrict__ b,
+                                T* __restrict__ scr, T rel, int maxiter, int nub, int nuf,
+                                int* status, T* sh)
 {
-    __shared__ T sh[32];
     const long long n = L.g.ncell();
     T* r = scr;
     T* rh = scr + n;
@@ -546,6 +733,153 @@ __global__ void k_mg_bottom(MGOp<T> L, T* __restrict__ x, const T* __restrict__ 
             __syncthreads();
         }
     if (tid == 0 && status) *status = ret;
+    __syncthreads();
+}
+
+template <typename T>
+__global__ void k_mg_bottom(MGOp<T> L, T* __restrict__ x, const T* __restrict__ b,
+                            T* __restrict__ scr, T rel, int maxiter, int nub, int nuf,
+                            int* status)
+{
+    if (mg_stopped(L)) return;
+    __shared__ T sh[32];
+    mg_bottom_block(L, x, b, scr, rel, maxiter, nub, nuf, status, sh);
+}
+
+// The coarse end of a V-cycle in one CTA: levels lc .. nl-1 (each at most a
+// few thousand cells) are smoothed, restricted, bottom-solved, prolongated
+// and smoothed again with block barriers between the sweeps, replacing
+// about ten kernel launches per level.  Level lc's right-hand side is
+// already restricted and its unknown zeroed.
+#define VD_MG_MAXLEV 16
+#define VD_MG_COARSE_SMEM (200 * 1024)
+template <typename T>
+struct MGCoarse
+{
+    int lc, nl;
+    MGOp<T> op[VD_MG_MAXLEV];
+    T* x[VD_MG_MAXLEV];
+    T* f[VD_MG_MAXLEV];
+};
+
+template <typename T>
+__device__ void mg_block_smooth(const MGOp<T>& L, T* __restrict__ x, const T* __restrict__ f,
+                                int nsm)
+{
+    const int nx = L.g.n[0], ny = L.g.n[1], nz = L.g.n[2];
+    const int nxh = (nx + 1) >> 1;
+    const int tot = nxh * ny * nz;
+    for (int sm = 0; sm < nsm; ++sm)
+        for (int color = 0; color < 2; ++color)
+        {
+            for (int t = threadIdx.x; t < tot; t += blockDim.x)
+            {
+                const int ih = t % nxh, r = t / nxh;
+                const int j = r % ny, k = r / ny;
+                const int i = 2 * ih + ((j + k + color) & 1);
+                if (i < nx) mg_gs_cell(L, x, f, i, j, k, false);
+            }
+            __syncthreads();
+        }
+}
+
+// Bytes of shared memory the coarse cycle needs to keep the unknowns and
+// right-hand sides of levels lc .. nl-1 and the bottom solver's six work
+// vectors on chip.
+template <typename T>
+size_t mg_coarse_smem(const MGCoarse<T>& C)
+{
+    size_t n = 0;
+    for (int l = C.lc; l < C.nl; ++l) n += 2 * (size_t)C.op[l].g.ncell();
+    n += 6 * (size_t)C.op[C.nl - 1].g.ncell();
+    return n * sizeof(T);
+}
+
+// With `on_chip`, every level's x and f live in dynamic shared memory (the
+// layout of mg_coarse_smem): level lc's right-hand side is read once from
+// global memory and its unknown written back once at the end.
+template <typename T>
+__global__ void __launch_bounds__(512) k_mg_coarse_vcycle(MGCoarse<T> C, T* __restrict__ scr,
+                                                          T rel, int maxiter, int nu1, int nu2,
+                                                          int nub, int nuf, int on_chip)
+{
+    extern __shared__ __align__(16) unsigned char mg_smem[];
+    if (mg_stopped(C.op[C.lc])) return;
+    __shared__ T sh[32];
+    const int last = C.nl - 1;
+    T* X[VD_MG_MAXLEV];
+    T* F[VD_MG_MAXLEV];
+    T* bscr = scr;
+    if (on_chip)
+    {
+        T* p = reinterpret_cast<T*>(mg_smem);
+        for (int l = C.lc; l <= last; ++l)
+        {
+            const long long n = C.op[l].g.ncell();
+            X[l] = p;
+            F[l] = p + n;
+            p += 2 * n;
+        }
+        bscr = p;
+        const long long n0 = C.op[C.lc].g.ncell();
+        for (long long q = threadIdx.x; q < n0; q += blockDim.x)
+        {
+            F[C.lc][q] = C.f[C.lc][q];
+            X[C.lc][q] = T(0);
+        }
+        __syncthreads();
+    } else
+        for (int l = C.lc; l <= last; ++l)
+        {
+            X[l] = C.x[l];
+            F[l] = C.f[l];
+        }
+    for (int l = C.lc; l < last; ++l)
+    {
+        const MGOp<T>& L = C.op[l];
+        mg_block_smooth(L, X[l], F[l], nu1);
+        const GridDev& gc = C.op[l + 1].g;
+        const int rz = (L.g.dim == 3) ? 2 : 1;
+        const T w = (L.g.dim == 3) ? T(0.125) : T(0.25);
+        for (long long c = threadIdx.x; c < gc.ncell(); c += blockDim.x)
+        {
+            const int I = (int)(c % gc.n[0]), J = (int)((c / gc.n[0]) % gc.n[1]),
+                      K = (int)(c / ((long long)gc.n[0] * gc.n[1]));
+            T s = T(0);
+            for (int kk = 0; kk < rz; ++kk)
+                for (int jj = 0; jj < 2; ++jj)
+                    for (int ii = 0; ii < 2; ++ii)
+                    {
+                        const int i = 2 * I + ii, j = 2 * J + jj, k = rz * K + kk;
+                        s += F[l][L.g.idx(i, j, k)] - mg_apply(L, X[l], i, j, k, false);
+                    }
+            const long long pc = gc.idx(I, J, K);
+            F[l + 1][pc] = s * w;
+            X[l + 1][pc] = T(0);
+        }
+        __syncthreads();
+    }
+    mg_bottom_block(C.op[last], X[last], F[last], bscr, rel, maxiter, nub, nuf, (int*)nullptr,
+                    sh);
+    for (int l = last - 1; l >= C.lc; --l)
+    {
+        const MGOp<T>& L = C.op[l];
+        const GridDev& gc = C.op[l + 1].g;
+        const int rz = (L.g.dim == 3) ? 2 : 1;
+        for (long long c = threadIdx.x; c < L.g.ncell(); c += blockDim.x)
+        {
+            const int i = (int)(c % L.g.n[0]), j = (int)((c / L.g.n[0]) % L.g.n[1]),
+                      k = (int)(c / ((long long)L.g.n[0] * L.g.n[1]));
+            X[l][L.g.idx(i, j, k)] += X[l + 1][gc.idx(i >> 1, j >> 1, k / rz)];
+        }
+        __syncthreads();
+        mg_block_smooth(L, X[l], F[l], nu2);
+    }
+    if (on_chip)
+    {
+        const long long n0 = C.op[C.lc].g.ncell();
+        for (long long q = threadIdx.x; q < n0; q += blockDim.x) C.x[C.lc][q] = X[C.lc][q];
+    }
 }
 
 // Mean of the coincident fine faces onto a coarse face.
@@ -629,4 +963,26 @@ __global__ void k_convert(TO* __restrict__ o, const TI* __restrict__ in, TI scal
         o[t] = (TO)(in[t] * scale);
 }
 
+} // namespace vd
+
+namespace vd {
+// Convergence bookkeeping of an asynchronous solve, on the device.
+struct MGDev
+{
+    unsigned long long rbits;      // max-norm of the latest residual
+    unsigned long long fbits;
+    unsigned long long final_bits; // residual after the last counted cycle
+    int done;
+    int iters;
+};
+
+// After each V-cycle: count it and raise the stop flag once the residual
+// meets the target (nothing happens once the flag is up).
+__global__ void k_mg_check(MGDev* s, double target)
+{
+    if (s->done) return;
+    s->iters += 1;
+    s->final_bits = s->rbits;
+    if (__longlong_as_double((long long)s->rbits) <= target) s->done = 1;
+}
 } // namespace vd

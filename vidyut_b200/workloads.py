@@ -11,6 +11,16 @@ N = 2.45e25 m^-3 at 300 K, WENO5-Z drift flux):
 * ``townsend_3d``: 3-D, 2 cm cube, 20 kV across z, Neumann on x and y, five
   seeded Gaussian blobs (peak log-uniform 1e16-1e19 m^-3, sigma uniform
   0.3-1 mm, centres uniform in the middle 60 % of the box), dt = 5e-13 s.
+* ``lmea``: the 8-species LMEA mechanism of ``vidyut_b200/mechgen.py``
+  (seed 2) with the electron-energy equation, 2 cm cube, 20 kV across z,
+  dt = 1e-12 s; initial ion, negative-ion and excited-neutral densities are
+  log-uniform 1e10-1e18 m^-3 per species, modulated by a smooth seeded
+  field, electrons set for quasi-neutrality, Te = 1 eV.
+* ``adjoint``: the ``lmea`` state with frozen analytic fields for the discrete
+  adjoint: E along -z of 1e6 V/m (times a smooth seeded factor in 0.5-1.5,
+  plus x/y components of a tenth of that), Te = 1 eV times a smooth seeded
+  factor in 0.75-1.25; gradients by the explicit flux + source steps at
+  dt = 1e-12 s.
 """
 from __future__ import annotations
 
@@ -99,4 +109,92 @@ def initial_state(cfg: Config, seed: int = 0) -> np.ndarray:
     S[info["etemp_id"]] = TE_LFA
     S[info["een_id"]] = 1.5 * n * K_B * TE_LFA
     S[info["cmask_id"]] = 1.0
+    return S
+
+
+TE_1EV = 11604.518
+
+
+def lmea_config(n: int, **kw) -> Config:
+    cfg = Config("lmea8")
+    cfg["dim"] = 3
+    cfg["n_cell"] = [n, n, n]
+    cfg["prob_hi"] = [0.02, 0.02, 0.02]
+    cfg["dt"] = 1e-12
+    cfg["hyp_order"] = 5
+    cfg["weno_scheme"] = 3
+    cfg["elecenergy_solve"] = 1
+    cfg["bound_specden"] = 1
+    cfg["min_species_density"] = 1.0
+    cfg["gas_temperature"] = TGAS
+    cfg["gas_pressure"] = NGAS * K_B * TGAS
+    cfg.set("vidyut.bg_species_ids", "6")
+    cfg["pot_bc_lo"] = [2, 2, 1]
+    cfg["pot_bc_hi"] = [2, 2, 1]
+    cfg["voltage_amp_hi"] = [0.0, 0.0, 20e3]
+    for k, v in kw.items():
+        cfg[k] = v
+    return cfg
+
+
+def lmea_state(cfg: Config, seed: int = 0) -> np.ndarray:
+    info = case_info(cfg.case)
+    nx, ny, nz = cfg["n_cell"]
+    rng = np.random.default_rng(seed)
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    z = (np.arange(nz) + 0.5) / nz
+
+    def smooth():
+        f = np.zeros((nz, ny, nx))
+        for _ in range(3):
+            kx, ky, kz = rng.integers(1, 4, size=3)
+            ph = rng.uniform(0, 2 * np.pi, size=3)
+            f += (np.cos(2 * np.pi * kz * z + ph[2])[:, None, None]
+                  * np.cos(2 * np.pi * ky * y + ph[1])[None, :, None]
+                  * np.cos(2 * np.pi * kx * x + ph[0])[None, None, :])
+        return 1.0 + 0.25 * f
+
+    S = np.zeros((info["nvar"], nz, ny, nx))
+    pos = [1, 2, 3, 4]
+    for s in pos:
+        S[s] = 10.0 ** rng.uniform(10.0, 18.0) * smooth()
+    S[5] = 0.5 * S[pos].sum(axis=0) * 10.0 ** rng.uniform(-8.0, 0.0)
+    S[0] = S[pos].sum(axis=0) - S[5]
+    S[6] = NGAS
+    S[7] = 10.0 ** rng.uniform(10.0, 18.0) * smooth()
+    S[info["etemp_id"]] = TE_1EV
+    S[info["een_id"]] = 1.5 * S[0] * K_B * TE_1EV
+    S[info["cmask_id"]] = 1.0
+    return S
+
+
+def adjoint_config(n: int, **kw) -> Config:
+    """The LMEA case as the adjoint runs it (clamped ghost cells, every
+    species BC Neumann so no wall zeroes a flux)."""
+    return lmea_config(n, **kw)
+
+
+def adjoint_state(cfg: Config, seed: int = 0, efield: float = 1e6) -> np.ndarray:
+    """``lmea_state`` plus the frozen E and Te fields of the adjoint runs."""
+    info = case_info(cfg.case)
+    S = lmea_state(cfg, seed)
+    nx, ny, nz = cfg["n_cell"]
+    rng = np.random.default_rng(seed + 1000)
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    z = (np.arange(nz) + 0.5) / nz
+
+    def wave():
+        kx, ky, kz = rng.integers(1, 3, size=3)
+        ph = rng.uniform(0, 2 * np.pi, size=3)
+        return (np.cos(2 * np.pi * kz * z + ph[2])[:, None, None]
+                * np.cos(2 * np.pi * ky * y + ph[1])[None, :, None]
+                * np.cos(2 * np.pi * kx * x + ph[0])[None, None, :])
+
+    ez = -efield * (1.0 + 0.5 * wave())
+    S[info["efx_id"]] = 0.1 * efield * wave()
+    S[info["efx_id"] + 1] = 0.1 * efield * wave()
+    S[info["efx_id"] + 2] = ez
+    S[info["etemp_id"]] = TE_1EV * (1.0 + 0.25 * wave())
     return S
