@@ -358,15 +358,80 @@ __global__ void __launch_bounds__(128) k_adj_chem_update(AdjParams P,
 
 #endif // VD_HAS_MECH_ADJOINT
 
-__global__ void k_adj_objective(long long n, const double* __restrict__ ue, double dv, double* J)
+// The objective sum_cells n_e dV is taken in double-double arithmetic
+// (Knuth's TwoSum on every addition) with a fixed reduction order: per-block
+// partials (hi, lo) first, then one block adds them up.  The result is the
+// exactly rounded sum up to a few units in the last place and the same on
+// every run, which central differences of the objective at h = 1e-6 need:
+// the objective reaches 1e10 while its sensitivities are 1e2, so one ulp of
+// J is worth ~2 in a difference quotient.
+__device__ __forceinline__ void dd_add(double& hi, double& lo, double b)
 {
-    __shared__ double sh[32];
-    double s = 0.0;
+    const double s = hi + b;
+    const double bb = s - hi;
+    lo += (hi - (s - bb)) + (b - bb);
+    hi = s;
+}
+
+__device__ __forceinline__ void dd_add_dd(double& hi, double& lo, double bh, double bl)
+{
+    dd_add(hi, lo, bh);
+    lo += bl;
+    const double s = hi + lo;
+    lo = lo - (s - hi);
+    hi = s;
+}
+
+// Block-wide double-double sum in a fixed order; thread 0 gets the result.
+__device__ __forceinline__ void dd_block_sum(double& hi, double& lo, double* sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        const double oh = __shfl_down_sync(0xffffffffu, hi, o);
+        const double ol = __shfl_down_sync(0xffffffffu, lo, o);
+        if (lane < o) dd_add_dd(hi, lo, oh, ol);
+    }
+    __syncthreads();
+    if (lane == 0)
+    {
+        sh[2 * wid] = hi;
+        sh[2 * wid + 1] = lo;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        const int nw = (blockDim.x + 31) >> 5;
+        for (int w = 1; w < nw; ++w) dd_add_dd(hi, lo, sh[2 * w], sh[2 * w + 1]);
+    }
+}
+
+// Stage 1: per-block partial sums of ue into part[2b], part[2b+1].
+__global__ void k_adj_objective(long long n, const double* __restrict__ ue,
+                                double* __restrict__ part)
+{
+    __shared__ double sh[64];
+    double hi = 0.0, lo = 0.0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x)
-        s += ue[t];
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) atomicAdd(J, s * dv);
+        dd_add(hi, lo, ue[t]);
+    dd_block_sum(hi, lo, sh);
+    if (threadIdx.x == 0)
+    {
+        part[2 * blockIdx.x] = hi;
+        part[2 * blockIdx.x + 1] = lo;
+    }
+}
+
+// Stage 2 (one block): J = dv * sum of the nb partials.
+__global__ void k_adj_objective_final(int nb, const double* __restrict__ part, double dv,
+                                      double* J)
+{
+    __shared__ double sh[64];
+    double hi = 0.0, lo = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) dd_add_dd(hi, lo, part[2 * b], part[2 * b + 1]);
+    dd_block_sum(hi, lo, sh);
+    if (threadIdx.x == 0) *J = (hi + lo) * dv;
 }
 
 } // namespace vd

@@ -997,6 +997,7 @@ struct AdjState
     double* adjnd = nullptr;
     double* theta = nullptr; // device log pre-factor shifts
     double* acc = nullptr;   // [0] J, [1..R] dJ/dtheta_r, [R+1] dJ/dscale
+    double* opart = nullptr; // per-block double-double partials of the objective
     double* hacc = nullptr;  // pinned mirror of acc
     std::vector<double> params; // theta_0 .. theta_{R-1}, electron mobility scale
     ~AdjState()
@@ -1038,6 +1039,7 @@ AdjState& adj_state(Ctx& c, int slots)
         a->adjnd = a->A.get<double>(N);
         a->theta = a->A.get<double>(ADJ_NR);
         a->acc = a->A.get<double>(ADJ_NR + 2);
+        a->opart = a->A.get<double>(2 * (size_t)gsz(N).x);
         VD_CUDA_OK(cudaMallocHost(&a->hacc, sizeof(double) * (ADJ_NR + 2)));
         a->params.assign(ADJ_NR + 1, 0.0);
         a->params[ADJ_NR] = 1.0;
@@ -1113,7 +1115,9 @@ double* adj_forward(Ctx& c, AdjState& a, const AdjParams& P, int nsteps, int K)
         adj_step(c, P, cur, nxt);
         cur = nxt;
     }
-    LAUNCH(k_adj_objective, gsz(N), BS, c.st, N, cur + (size_t)a.eslot * N,
+    const dim3 gob = gsz(N);
+    LAUNCH(k_adj_objective, gob, BS, c.st, N, cur + (size_t)a.eslot * N, a.opart);
+    LAUNCH(k_adj_objective_final, 1, 1024, c.st, (int)gob.x, (const double*)a.opart,
            adj_cell_volume(c), a.acc);
     return cur;
 }
