@@ -254,9 +254,28 @@ void hier_coarsen_coeffs(Hier<T>& H, const int* bct, cudaStream_t st)
     }
 }
 
+// 3-D red-black split levels with no periodic direction run the kernels
+// that keep several planes per thread in flight (k_mg_sweep3, k_mg_restrict3,
+// k_mg_resid3).
+template <typename T>
+bool mg3_ok(const MGOp<T>& op)
+{
+    const GridDev& g = op.g;
+    return g.rb && g.dim == 3 && g.n[0] >= 4 && g.n[1] >= 4 && g.n[2] >= 4 && !op.a &&
+           !g.per[0] && !g.per[1] && !g.per[2] && g.ncell() < (1LL << 31);
+}
+
+dim3 mg3_grid(const GridDev& g)
+{
+    return dim3((g.n[0] / 2 + 31) / 32, (g.n[1] + 7) / 8, (g.n[2] + MG3_U - 1) / MG3_U);
+}
+
+// n Gauss-Seidel iterations (colour 0, colour 1).  With xc given (only for
+// mg3_ok levels) the first colour-0 sweep also adds the prolongated coarse
+// correction xc of level gc.
 template <typename T>
 void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t st,
-            int prof_tag = VD_PROF_NONE)
+            int prof_tag = VD_PROF_NONE, const GridDev* gc = nullptr, const T* xc = nullptr)
 {
     const long long half = (long long)((op.g.n[0] + 1) / 2) * op.g.n[1] * op.g.n[2];
     const bool prof = t_prof && prof_tag != VD_PROF_NONE && t_prof->id == prof_tag;
@@ -271,8 +290,40 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
             if (prof) t_prof->begin(st);
             T gamma = op.aconst; // interior diagonal of the constant-coefficient operator
             for (int d = 0; d < op.g.dim; ++d) gamma += op.dh[d] * (op.bconst + op.bconst);
-            if (op.g.rb && op.g.dim == 3 && op.g.n[0] >= 4 && op.g.n[1] >= 4 &&
-                op.g.n[2] >= 4 && !op.a)
+            if (mg3_ok(op))
+            {
+                const dim3 grid = mg3_grid(op.g);
+                const bool pro = xc && s == 0 && color == 0;
+                const GridDev gcv = gc ? *gc : op.g;
+                if (!pro && op.g.n[0] % 4 == 0)
+                {
+                    // pairs of half-cells per thread, 16-byte accesses
+                    const dim3 gv((op.g.n[0] / 2 + 63) / 64, grid.y, grid.z);
+                    if (op.b[0])
+                        LAUNCH((k_mg_sweep3v<T, true>), gv, 256, st, op, x, f, color,
+                               inh ? 1 : 0, T(0));
+                    else
+                        LAUNCH((k_mg_sweep3v<T, false>), gv, 256, st, op, x, f, color,
+                               inh ? 1 : 0, T(1) / gamma);
+                } else if (op.b[0])
+                {
+                    if (pro)
+                        LAUNCH((k_mg_sweep3<T, true, true>), grid, 256, st, op, x, f, color,
+                               inh ? 1 : 0, T(0), gcv, xc);
+                    else
+                        LAUNCH((k_mg_sweep3<T, true, false>), grid, 256, st, op, x, f, color,
+                               inh ? 1 : 0, T(0), gcv, xc);
+                } else
+                {
+                    if (pro)
+                        LAUNCH((k_mg_sweep3<T, false, true>), grid, 256, st, op, x, f, color,
+                               inh ? 1 : 0, T(1) / gamma, gcv, xc);
+                    else
+                        LAUNCH((k_mg_sweep3<T, false, false>), grid, 256, st, op, x, f, color,
+                               inh ? 1 : 0, T(1) / gamma, gcv, xc);
+                }
+            } else if (op.g.rb && op.g.dim == 3 && op.g.n[0] >= 4 && op.g.n[1] >= 4 &&
+                       op.g.n[2] >= 4 && !op.a)
             {
                 const int nxh = op.g.n[0] / 2;
                 const int bx = nxh >= 128 ? 128 : (nxh >= 64 ? 64 : (nxh >= 32 ? 32 : 16));
@@ -346,6 +397,18 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         T* fl = l ? H.f[l] : f0;
         const bool inh = (l == 0) && inh0;
         smooth(H.op[l], xl, fl, inh, H.nu1, st, l == 0 ? H.prof_tag : VD_PROF_NONE);
+        if (mg3_ok(H.op[l]))
+        {
+            const GridDev& gc = H.g[l + 1];
+            const dim3 grid((gc.n[0] + 31) / 32, (gc.n[1] + 7) / 8, gc.n[2]);
+            if (H.op[l].b[0])
+                LAUNCH((k_mg_restrict3<T, true>), grid, 256, st, H.op[l], xl, fl, gc,
+                       H.f[l + 1], H.x[l + 1], inh ? 1 : 0);
+            else
+                LAUNCH((k_mg_restrict3<T, false>), grid, 256, st, H.op[l], xl, fl, gc,
+                       H.f[l + 1], H.x[l + 1], inh ? 1 : 0);
+            continue;
+        }
         const Grid3 gr = rows3(H.g[l + 1]);
         LAUNCH(k_mg_resid_restrict<T>, gr.g, gr.b, st, H.op[l], xl, fl, H.g[l + 1], H.f[l + 1],
                H.x[l + 1], inh ? 1 : 0);
@@ -377,6 +440,12 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         T* xl = l ? H.x[l] : x0;
         T* fl = l ? H.f[l] : f0;
         const bool inh = (l == 0) && inh0;
+        if (mg3_ok(H.op[l]) && H.nu2 >= 1)
+        {
+            smooth(H.op[l], xl, fl, inh, H.nu2, st, l == 0 ? H.prof_tag : VD_PROF_NONE,
+                   &H.g[l + 1], (const T*)H.x[l + 1]);
+            continue;
+        }
         const Grid3 gp = rows3(H.g[l]);
         LAUNCH(k_mg_prolong_add<T>, gp.g, gp.b, st, H.g[l], H.g[l + 1], xl, H.x[l + 1],
                H.op[l].stop);
@@ -504,8 +573,24 @@ double read_norm(Ctx& c)
 // the bit patterns at mx[0] (|r|) and mx[1] (|f| when `fnorm`).
 template <typename T>
 void launch_norm(Ctx& c, const MGOp<T>& op, const T* x, const T* f, T* rout, bool inh,
-                 bool fnorm, unsigned long long* mx)
+                 bool fnorm, unsigned long long* mx, bool both = true)
 {
+    if (mg3_ok(op))
+    {
+        const dim3 grid = mg3_grid(op.g);
+        const long long nb = (long long)grid.x * grid.y * grid.z;
+        if (nb <= c.npart)
+        {
+            if (op.b[0])
+                LAUNCH((k_mg_resid3<T, true>), grid, 256, c.st, op, x, f, rout, inh ? 1 : 0,
+                       both ? 1 : 0, fnorm ? 1 : 0, c.dpart);
+            else
+                LAUNCH((k_mg_resid3<T, false>), grid, 256, c.st, op, x, f, rout, inh ? 1 : 0,
+                       both ? 1 : 0, fnorm ? 1 : 0, c.dpart);
+            LAUNCH(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nb, fnorm ? 1 : 0, mx);
+            return;
+        }
+    }
     if (op.g.rb)
     {
         const long long half = op.g.ncell() >> 1;
@@ -649,8 +734,10 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
                 for (int b = 0; b < nb; ++b)
                 {
                     vcycle(H64, sol, rhs, true, c.dscal, c.st);
+                    // the cycle ends with a colour-1 sweep of level 0, whose
+                    // cells then have no residual: only colour 0 is scanned
                     launch_norm(c, op0, (const double*)sol, (const double*)rhs, (double*)nullptr,
-                                true, false, &c.dmg->rbits);
+                                true, false, &c.dmg->rbits, H64.nu2 < 1);
                     LAUNCH(k_mg_check, 1, 1, c.st, c.dmg, target);
                     ++issued;
                 }

@@ -376,6 +376,703 @@ __global__ void __launch_bounds__(256) k_mg_smooth_rb3(MGOp<T> L, T* __restrict_
         xs[h] = (fv + rho) * inv_gamma;
 }
 
+// ---------------------------------------------------------------------
+// 3-D red-black split levels, several planes per thread.  A thread owns
+// half-cell ih of row j in MG3_U consecutive planes and issues every load
+// of those cells before any arithmetic (the loads of one sweep are the
+// bytes in flight that HBM bandwidth needs); the stop flag is read in
+// parallel with them and only gates the stores.  Every cell takes the same
+// code: a neighbour outside the level is replaced by its ghost value
+// c0 x0 + c1 x1 + g (x1 the neighbour on the opposite side, loaded in its
+// place), so the cells next to the boundary cost a few selects instead of
+// a divergent general path.  Warps with no such cell skip even those.
+
+#define MG3_U 2
+
+// Boundary data of side s = d + 3 (hi) at plane index p: c0, c1 and the
+// inhomogeneous part g of the ghost closure.
+template <typename T>
+__device__ __forceinline__ void mg3_ghost(const MGOp<T>& L, int s, int p, bool inhomog, T& c0,
+                                          T& c1, T& gv)
+{
+    c0 = L.c0[s] ? L.c0[s][p] : L.c0s[s];
+    c1 = L.c1s[s];
+    gv = (inhomog && L.gv[s]) ? L.gv[s][p] : T(0);
+}
+
+// Face coefficients b[0..5] = x-lo, x-hi, y-lo, y-hi, z-lo, z-hi of cell (i,j,k).
+template <typename T, bool VARB>
+__device__ __forceinline__ void mg3_faces(const MGOp<T>& L, int i, int j, int k, T* b)
+{
+    if (!VARB)
+    {
+#pragma unroll
+        for (int m = 0; m < 6; ++m) b[m] = L.bconst;
+        return;
+    }
+    const int nx = L.g.n[0], ny = L.g.n[1];
+    const long long r = j + (long long)ny * k;
+    const long long fx = i + (long long)(nx + 1) * r;
+    b[0] = __ldg(L.b[0] + fx);
+    b[1] = __ldg(L.b[0] + fx + 1);
+    const long long fy = i + (long long)nx * (j + (long long)(ny + 1) * k);
+    b[2] = __ldg(L.b[1] + fy);
+    b[3] = __ldg(L.b[1] + fy + nx);
+    const long long fz = i + (long long)nx * r;
+    b[4] = __ldg(L.b[2] + fz);
+    b[5] = __ldg(L.b[2] + fz + (long long)nx * ny);
+}
+
+// Offsets (relative to the cell's half-index h in the other colour) of
+// the six neighbours x-lo, x-hi, y-lo, y-hi, z-lo, z-hi; a neighbour outside
+// the level takes the offset of the opposite one (a valid address whose
+// value the ghost closure needs anyway).  Returns the mask of outside sides.
+__device__ __forceinline__ int mg3_offsets(const GridDev& g, int i, int j, int k, int q,
+                                           long long* off)
+{
+    const long long nxh = g.n[0] >> 1, plane = nxh * g.n[1];
+    const int out = (i == 0) | ((i == g.n[0] - 1) << 1) | ((j == 0) << 2) |
+                    ((j == g.n[1] - 1) << 3) | ((k == 0) << 4) | ((k == g.n[2] - 1) << 5);
+    off[0] = q - 1;
+    off[1] = q;
+    off[2] = -nxh;
+    off[3] = nxh;
+    off[4] = -plane;
+    off[5] = plane;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+        if (out & (1 << (2 * d))) off[2 * d] = off[2 * d + 1];
+        if (out & (2 << (2 * d))) off[2 * d + 1] = off[2 * d];
+    }
+    return out;
+}
+
+// Replace the outside neighbours in nb by their ghost part c1 x1 + g and
+// return sum_d dh_d b_side c0 (the ghost's share of x0, absorbed into the
+// diagonal).  x1 of an outside side is the opposite neighbour.
+template <typename T>
+__device__ __forceinline__ T mg3_apply_ghosts(const MGOp<T>& L, int out, int i, int j, int k,
+                                              bool inhomog, const T* b, T* nb)
+{
+    T delta = T(0);
+#pragma unroll
+    for (int s2 = 0; s2 < 6; ++s2)
+    {
+        if (!(out & (1 << s2))) continue;
+        const int d = s2 >> 1, hi = s2 & 1;
+        const int s = d + 3 * hi;
+        const int p = (d == 0) ? (j + L.g.n[1] * k) : ((d == 1) ? (i + L.g.n[0] * k) : (i + L.g.n[0] * j));
+        T c0, c1, gv;
+        mg3_ghost(L, s, p, inhomog, c0, c1, gv);
+        nb[s2] = c1 * nb[s2 ^ 1] + gv;
+        delta += L.dh[d] * (b[s2] * c0);
+    }
+    return delta;
+}
+
+// One colour of Gauss-Seidel on a 3-D red-black split level (nx even, all
+// sizes >= 4, no periodic direction); 256-thread blocks of 32 half-cells by
+// 8 rows, grid z over plane groups of MG3_U.  With PROL the other colour is
+// read as x + P e (e the coarse correction, P piecewise constant): the
+// post-smoothing's first sweep takes the place of the separate
+// prolongation pass, which is exact because a Gauss-Seidel value does not
+// depend on the cell's own previous value.
+//   interior:  x = (f + sum_d dh_d (b_lo x_lo + b_hi x_hi)) / gamma
+//   boundary:  the same with ghost parts in the sum and gamma - delta.
+template <typename T, bool VARB, bool PROL>
+__global__ void __launch_bounds__(256, 4) k_mg_sweep3(const __grid_constant__ MGOp<T> L,
+                                                      T* __restrict__ x,
+                                                      const T* __restrict__ f, int color,
+                                                      int inhomog, T inv_gamma, GridDev gc,
+                                                      const T* __restrict__ xc)
+{
+    const int stop = L.stop ? *(volatile const int*)L.stop : 0;
+    const GridDev& g = L.g;
+    const int nx = g.n[0], nxh = nx >> 1, ny = g.n[1], nz = g.n[2];
+    const int ih = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int k0 = blockIdx.z * MG3_U;
+    const bool active = ih < nxh && j < ny;
+    const long long half = g.ncell() >> 1;
+    T* __restrict__ xs = x + color * half;
+    const T* __restrict__ xo = x + (1 - color) * half;
+    const T* __restrict__ fs = f + color * half;
+    const T dhx = L.dh[0], dhy = L.dh[1], dhz = L.dh[2];
+    // warps that touch no boundary cell (nor a partial row) take straight-line
+    // code with fixed neighbour offsets (32-bit: half < 2^31 on these levels)
+    // (the x ends of each row are in the fast path: their one outside
+    // neighbour is the ghost of side x-lo / x-hi)
+    const bool edge = active && (j == 0 || j == ny - 1 || k0 == 0 || k0 + MG3_U > nz - 1);
+    if (!__any_sync(0xffffffffu, edge))
+    {
+        if (!active) return;
+        const int plane = nxh * ny;
+        const int hb = ih + nxh * (j + ny * k0);
+        T v[MG3_U][7];
+#pragma unroll
+        for (int u = 0; u < MG3_U; ++u)
+        {
+            const int q = (j + k0 + u + color) & 1;
+            const int h = hb + u * plane;
+            const int i = 2 * ih + q;
+            const int xlo = i == 0, xhi = i == nx - 1;
+            v[u][0] = __ldg(xo + (h + q - 1 + xlo));
+            v[u][1] = __ldg(xo + (h + q - xhi));
+            v[u][2] = __ldg(xo + (h - nxh));
+            v[u][3] = __ldg(xo + (h + nxh));
+            v[u][4] = __ldg(xo + (h - plane));
+            v[u][5] = __ldg(xo + (h + plane));
+            v[u][6] = __ldg(fs + h);
+            if (PROL)
+            {
+                const int k = k0 + u, I = i >> 1, J = j >> 1, K = k >> 1;
+                v[u][0] += __ldg(xc + gc.idx((xlo ? i + 1 : i - 1) >> 1, J, K));
+                v[u][1] += __ldg(xc + gc.idx((xhi ? i - 1 : i + 1) >> 1, J, K));
+                v[u][2] += __ldg(xc + gc.idx(I, (j - 1) >> 1, K));
+                v[u][3] += __ldg(xc + gc.idx(I, (j + 1) >> 1, K));
+                v[u][4] += __ldg(xc + gc.idx(I, J, (k - 1) >> 1));
+                v[u][5] += __ldg(xc + gc.idx(I, J, (k + 1) >> 1));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < MG3_U; ++u)
+        {
+            const int q = (j + k0 + u + color) & 1;
+            const int i = 2 * ih + q;
+            const int xo_ = (i == 0) ? 1 : ((i == nx - 1) ? 2 : 0);
+            T b[6];
+            mg3_faces<T, VARB>(L, i, j, k0 + u, b);
+            T delta = T(0);
+            if (xo_) delta = mg3_apply_ghosts(L, xo_, i, j, k0 + u, inhomog != 0, b, v[u]);
+            T out;
+            if (!VARB)
+            {
+                const T cb = L.bconst;
+                T rho = (dhx * cb) * (v[u][0] + v[u][1]);
+                rho = fma(dhy * cb, v[u][2] + v[u][3], rho);
+                rho = fma(dhz * cb, v[u][4] + v[u][5], rho);
+                if (!xo_)
+                    out = (v[u][6] + rho) * inv_gamma;
+                else
+                {
+                    T gamma = L.aconst;
+                    gamma += dhx * (cb + cb);
+                    gamma += dhy * (cb + cb);
+                    gamma += dhz * (cb + cb);
+                    out = (v[u][6] + rho) / (gamma - delta);
+                }
+            } else
+            {
+                T rho = dhx * (b[0] * v[u][0] + b[1] * v[u][1]);
+                rho += dhy * (b[2] * v[u][2] + b[3] * v[u][3]);
+                rho += dhz * (b[4] * v[u][4] + b[5] * v[u][5]);
+                T gamma = L.aconst;
+                gamma += dhx * (b[0] + b[1]);
+                gamma += dhy * (b[2] + b[3]);
+                gamma += dhz * (b[4] + b[5]);
+                out = (v[u][6] + rho) / (gamma - delta);
+            }
+            if (!stop) xs[hb + u * (nxh * ny)] = out;
+        }
+        return;
+    }
+    if (!active) return;
+    T v[MG3_U][7];
+    int outm[MG3_U];
+    long long hh[MG3_U];
+#pragma unroll
+    for (int u = 0; u < MG3_U; ++u)
+    {
+        const int k = min(k0 + u, nz - 1);
+        const int q = (j + k + color) & 1;
+        const int i = 2 * ih + q;
+        long long off[6];
+        outm[u] = mg3_offsets(g, i, j, k, q, off);
+        const long long h = ih + (long long)nxh * (j + (long long)ny * k);
+        hh[u] = h;
+#pragma unroll
+        for (int m = 0; m < 6; ++m) v[u][m] = __ldg(xo + h + off[m]);
+        v[u][6] = __ldg(fs + h);
+        if (PROL)
+        {
+            // coarse corrections of the neighbours' parent cells (the
+            // coarse level may be in either layout)
+            const int ci[6] = {i - 1, i + 1, i, i, i, i}, cj[6] = {j, j, j - 1, j + 1, j, j},
+                      ck[6] = {k, k, k, k, k - 1, k + 1};
+#pragma unroll
+            for (int m = 0; m < 6; ++m)
+            {
+                const int mm = (outm[u] & (1 << m)) ? (m ^ 1) : m;
+                v[u][m] += __ldg(xc + gc.idx(ci[mm] >> 1, cj[mm] >> 1, ck[mm] >> 1));
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < MG3_U; ++u)
+    {
+        const int k = k0 + u;
+        if (k >= nz) break;
+        const int q = (j + k + color) & 1;
+        const int i = 2 * ih + q;
+        T b[6];
+        mg3_faces<T, VARB>(L, i, j, k, b);
+        T delta = T(0);
+        if (outm[u]) delta = mg3_apply_ghosts(L, outm[u], i, j, k, inhomog != 0, b, v[u]);
+        T out;
+        if (!VARB)
+        {
+            const T cb = L.bconst;
+            T rho = (dhx * cb) * (v[u][0] + v[u][1]);
+            rho = fma(dhy * cb, v[u][2] + v[u][3], rho);
+            rho = fma(dhz * cb, v[u][4] + v[u][5], rho);
+            if (delta == T(0))
+                out = (v[u][6] + rho) * inv_gamma;
+            else
+            {
+                T gamma = L.aconst; // as the host forms the interior diagonal
+                gamma += dhx * (cb + cb);
+                gamma += dhy * (cb + cb);
+                gamma += dhz * (cb + cb);
+                out = (v[u][6] + rho) / (gamma - delta);
+            }
+        } else
+        {
+            T rho = dhx * (b[0] * v[u][0] + b[1] * v[u][1]);
+            rho += dhy * (b[2] * v[u][2] + b[3] * v[u][3]);
+            rho += dhz * (b[4] * v[u][4] + b[5] * v[u][5]);
+            T gamma = L.aconst;
+            gamma += dhx * (b[0] + b[1]);
+            gamma += dhy * (b[2] + b[3]);
+            gamma += dhz * (b[4] + b[5]);
+            out = (v[u][6] + rho) / (gamma - delta);
+        }
+        if (!stop) xs[hh[u]] = out;
+    }
+}
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double>
+{
+    using type = double2;
+};
+template <>
+struct Vec2<float>
+{
+    using type = float2;
+};
+
+// Gauss-Seidel value of one cell from its six neighbour values (outside
+// ones still to be replaced by ghosts when `out` is non-zero) and f.
+template <typename T, bool VARB>
+__device__ __forceinline__ T mg3_gs_value(const MGOp<T>& L, int i, int j, int k, int out,
+                                          bool inhomog, T inv_gamma, T fv, T* nb)
+{
+    T b[6];
+    mg3_faces<T, VARB>(L, i, j, k, b);
+    T delta = T(0);
+    if (out) delta = mg3_apply_ghosts(L, out, i, j, k, inhomog, b, nb);
+    const T dhx = L.dh[0], dhy = L.dh[1], dhz = L.dh[2];
+    if (!VARB)
+    {
+        const T cb = L.bconst;
+        T rho = (dhx * cb) * (nb[0] + nb[1]);
+        rho = fma(dhy * cb, nb[2] + nb[3], rho);
+        rho = fma(dhz * cb, nb[4] + nb[5], rho);
+        if (!out) return (fv + rho) * inv_gamma;
+        T gamma = L.aconst; // as the host forms the interior diagonal
+        gamma += dhx * (cb + cb);
+        gamma += dhy * (cb + cb);
+        gamma += dhz * (cb + cb);
+        return (fv + rho) / (gamma - delta);
+    }
+    T rho = dhx * (b[0] * nb[0] + b[1] * nb[1]);
+    rho += dhy * (b[2] * nb[2] + b[3] * nb[3]);
+    rho += dhz * (b[4] * nb[4] + b[5] * nb[5]);
+    T gamma = L.aconst;
+    gamma += dhx * (b[0] + b[1]);
+    gamma += dhy * (b[2] + b[3]);
+    gamma += dhz * (b[4] + b[5]);
+    return (fv + rho) / (gamma - delta);
+}
+
+// One colour of Gauss-Seidel, two adjacent half-cells per thread with
+// 16-byte (two-element) loads and stores: of a pair's x neighbours three
+// are distinct (one vector and one scalar load), and its y, z neighbours
+// and f are vectors.  Needs nx % 4 == 0 (pairs never straddle a row and
+// rows start 16-byte aligned).  Blocks of 32 pairs by 8 rows, MG3_U planes
+// per thread; warps with a row or plane on the level boundary update their
+// cells one by one with the ghost closure.
+template <typename T, bool VARB>
+__global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ MGOp<T> L,
+                                                       T* __restrict__ x,
+                                                       const T* __restrict__ f, int color,
+                                                       int inhomog, T inv_gamma)
+{
+    using V2 = typename Vec2<T>::type;
+    const int stop = L.stop ? *(volatile const int*)L.stop : 0;
+    const GridDev& g = L.g;
+    const int nx = g.n[0], nxh = nx >> 1, ny = g.n[1], nz = g.n[2];
+    const int pr = blockIdx.x * 32 + (threadIdx.x & 31); // pair index: half-cells 2pr, 2pr+1
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int k0 = blockIdx.z * MG3_U;
+    const bool active = 2 * pr < nxh && j < ny;
+    const long long half = g.ncell() >> 1;
+    T* __restrict__ xs = x + color * half;
+    const T* __restrict__ xo = x + (1 - color) * half;
+    const T* __restrict__ fs = f + color * half;
+    const bool edge = active && (j == 0 || j == ny - 1 || k0 == 0 || k0 + MG3_U > nz - 1);
+    if (!__any_sync(0xffffffffu, edge))
+    {
+        if (!active) return;
+        const int plane = nxh * ny;
+        const int hb = 2 * pr + nxh * (j + ny * k0);
+        V2 vx[MG3_U], vym[MG3_U], vyp[MG3_U], vzm[MG3_U], vzp[MG3_U], vf[MG3_U];
+        T sx[MG3_U];
+#pragma unroll
+        for (int u = 0; u < MG3_U; ++u)
+        {
+            const int q = (j + k0 + u + color) & 1;
+            const int h = hb + u * plane;
+            // the pair's outer x neighbour: 2pr-1 (q = 0) or 2pr+2 (q = 1);
+            // at the ends of a row the ghost closure replaces it
+            const bool xlo = q == 0 && pr == 0, xhi = q == 1 && 2 * pr + 2 == nxh;
+            const int so = q ? (xhi ? 1 : 2) : (xlo ? 0 : -1);
+            vx[u] = __ldg(reinterpret_cast<const V2*>(xo + h));
+            sx[u] = __ldg(xo + h + so);
+            vym[u] = __ldg(reinterpret_cast<const V2*>(xo + h - nxh));
+            vyp[u] = __ldg(reinterpret_cast<const V2*>(xo + h + nxh));
+            vzm[u] = __ldg(reinterpret_cast<const V2*>(xo + h - plane));
+            vzp[u] = __ldg(reinterpret_cast<const V2*>(xo + h + plane));
+            vf[u] = __ldg(reinterpret_cast<const V2*>(fs + h));
+        }
+#pragma unroll
+        for (int u = 0; u < MG3_U; ++u)
+        {
+            const int k = k0 + u;
+            const int q = (j + k + color) & 1;
+            const int iA = 4 * pr + q, iB = iA + 2;
+            T nA[6], nB[6];
+            if (q == 0)
+            {
+                nA[0] = sx[u];
+                nA[1] = vx[u].x;
+                nB[0] = vx[u].x;
+                nB[1] = vx[u].y;
+            } else
+            {
+                nA[0] = vx[u].x;
+                nA[1] = vx[u].y;
+                nB[0] = vx[u].y;
+                nB[1] = sx[u];
+            }
+            nA[2] = vym[u].x;
+            nB[2] = vym[u].y;
+            nA[3] = vyp[u].x;
+            nB[3] = vyp[u].y;
+            nA[4] = vzm[u].x;
+            nB[4] = vzm[u].y;
+            nA[5] = vzp[u].x;
+            nB[5] = vzp[u].y;
+            const int oA = (iA == 0) ? 1 : 0, oB = (iB == nx - 1) ? 2 : 0;
+            V2 o;
+            o.x = mg3_gs_value<T, VARB>(L, iA, j, k, oA, inhomog != 0, inv_gamma, vf[u].x, nA);
+            o.y = mg3_gs_value<T, VARB>(L, iB, j, k, oB, inhomog != 0, inv_gamma, vf[u].y, nB);
+            if (!stop) *reinterpret_cast<V2*>(xs + hb + u * plane) = o;
+        }
+        return;
+    }
+    if (!active) return;
+    // boundary rows and planes: cell by cell
+#pragma unroll 1
+    for (int u = 0; u < MG3_U; ++u)
+    {
+        const int k = k0 + u;
+        if (k >= nz) break;
+        for (int e = 0; e < 2; ++e)
+        {
+            const int ih = 2 * pr + e;
+            const int q = (j + k + color) & 1;
+            const int i = 2 * ih + q;
+            long long off[6];
+            const int out = mg3_offsets(g, i, j, k, q, off);
+            const long long h = ih + (long long)nxh * (j + (long long)ny * k);
+            T nb[6];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) nb[m] = __ldg(xo + h + off[m]);
+            const T v = mg3_gs_value<T, VARB>(L, i, j, k, out, inhomog != 0, inv_gamma,
+                                              __ldg(fs + h), nb);
+            if (!stop) xs[h] = v;
+        }
+    }
+}
+
+// Residual f - L(x) of one cell from its value x0 and neighbour values nb
+// (outside ones replaced in place by their ghost parts; the ghost's c0 x0
+// share enters through delta): mg_apply's operator.
+template <typename T>
+__device__ __forceinline__ T mg3_residual(const MGOp<T>& L, T fv, T x0, T* nb, const T* b,
+                                          int out, int i, int j, int k, bool inhomog)
+{
+    if (out)
+    {
+#pragma unroll
+        for (int s2 = 0; s2 < 6; ++s2)
+        {
+            if (!(out & (1 << s2))) continue;
+            const int d = s2 >> 1, hi = s2 & 1;
+            const int s = d + 3 * hi;
+            const int p = (d == 0) ? (j + L.g.n[1] * k) : ((d == 1) ? (i + L.g.n[0] * k) : (i + L.g.n[0] * j));
+            T c0, c1, gv;
+            mg3_ghost(L, s, p, inhomog, c0, c1, gv);
+            nb[s2] = c0 * x0 + (c1 * nb[s2 ^ 1] + gv);
+        }
+    }
+    T y = L.aconst * x0;
+    y -= L.dh[0] * (b[1] * (nb[1] - x0) - b[0] * (x0 - nb[0]));
+    y -= L.dh[1] * (b[3] * (nb[3] - x0) - b[2] * (x0 - nb[2]));
+    y -= L.dh[2] * (b[5] * (nb[5] - x0) - b[4] * (x0 - nb[4]));
+    return fv - y;
+}
+
+// Residual f - L(x) at the 8 children of every coarse cell, averaged into
+// the coarse right-hand side (order kk, jj, ii as k_mg_resid_restrict); the
+// coarse unknown zeroed.  3-D red-black split fine level; blocks of 32
+// coarse cells in x by 8 coarse rows, one coarse plane per grid z.
+template <typename T, bool VARB>
+__global__ void __launch_bounds__(256, 3) k_mg_restrict3(const __grid_constant__ MGOp<T> L,
+                                                      const T* __restrict__ x,
+                                                      const T* __restrict__ f, GridDev gc,
+                                                      T* __restrict__ fc, T* __restrict__ xc,
+                                                      int inhomog)
+{
+    const int stop = L.stop ? *(volatile const int*)L.stop : 0;
+    const GridDev& g = L.g;
+    const int nxh = g.n[0] >> 1, ny = g.n[1];
+    const int I = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int J = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int K = blockIdx.z;
+    const bool active = I < gc.n[0] && J < gc.n[1];
+    const long long half = g.ncell() >> 1;
+    T s = T(0);
+    const bool edge = active && (J == 0 || J == gc.n[1] - 1 || K == 0 || K == gc.n[2] - 1);
+    if (!__any_sync(0xffffffffu, edge))
+    {
+        if (!active) return;
+        // no child on the level boundary: fixed offsets, 32-bit indices
+        const int plane = nxh * ny;
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk)
+        {
+            T xv[4][8];
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+                for (int ii = 0; ii < 2; ++ii)
+                {
+                    const int m = ii + 2 * jj;
+                    const int c = (ii + jj + kk) & 1;
+                    const int h = I + nxh * (2 * J + jj + ny * (2 * K + kk));
+                    const T* xs = x + c * half;
+                    const T* xo = x + (1 - c) * half;
+                    const int i = 2 * I + ii;
+                    const int xlo = i == 0, xhi = i == g.n[0] - 1;
+                    xv[m][0] = __ldg(xo + (h + ii - 1 + xlo));
+                    xv[m][1] = __ldg(xo + (h + ii - xhi));
+                    xv[m][2] = __ldg(xo + (h - nxh));
+                    xv[m][3] = __ldg(xo + (h + nxh));
+                    xv[m][4] = __ldg(xo + (h - plane));
+                    xv[m][5] = __ldg(xo + (h + plane));
+                    xv[m][6] = __ldg(xs + h);
+                    xv[m][7] = __ldg(f + c * half + h);
+                }
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+                for (int ii = 0; ii < 2; ++ii)
+                {
+                    const int m = ii + 2 * jj;
+                    const int i = 2 * I + ii;
+                    const int xo_ = (i == 0) ? 1 : ((i == g.n[0] - 1) ? 2 : 0);
+                    T b[6];
+                    mg3_faces<T, VARB>(L, i, 2 * J + jj, 2 * K + kk, b);
+                    s += mg3_residual(L, xv[m][7], xv[m][6], xv[m], b, xo_, i, 2 * J + jj,
+                                      2 * K + kk, inhomog != 0);
+                }
+        }
+        if (stop) return;
+        const long long pc = gc.idx(I, J, K);
+        fc[pc] = s * T(0.125);
+        xc[pc] = T(0);
+        return;
+    }
+    if (!active) return;
+#pragma unroll
+    for (int kk = 0; kk < 2; ++kk)
+    {
+        // the four children of this plane: every load first
+        T xv[4][8];
+        int outm[4];
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+            for (int ii = 0; ii < 2; ++ii)
+            {
+                const int m = ii + 2 * jj;
+                const int i = 2 * I + ii, j = 2 * J + jj, k = 2 * K + kk;
+                const int c = (ii + jj + kk) & 1;
+                long long off[6];
+                outm[m] = mg3_offsets(g, i, j, k, ii, off);
+                const long long h = I + (long long)nxh * (j + (long long)ny * k);
+                const T* xs = x + c * half;
+                const T* xo = x + (1 - c) * half;
+                xv[m][6] = __ldg(xs + h);
+#pragma unroll
+                for (int d = 0; d < 6; ++d) xv[m][d] = __ldg(xo + h + off[d]);
+                xv[m][7] = __ldg(f + c * half + h);
+            }
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+            for (int ii = 0; ii < 2; ++ii)
+            {
+                const int m = ii + 2 * jj;
+                const int i = 2 * I + ii, j = 2 * J + jj, k = 2 * K + kk;
+                T b[6];
+                mg3_faces<T, VARB>(L, i, j, k, b);
+                s += mg3_residual(L, xv[m][7], xv[m][6], xv[m], b, outm[m], i, j, k,
+                                  inhomog != 0);
+            }
+    }
+    if (stop) return;
+    const long long pc = gc.idx(I, J, K);
+    fc[pc] = s * T(0.125);
+    xc[pc] = T(0);
+}
+
+// Residual max-norm on a 3-D red-black split level: cells of colour 0 only
+// (after a sweep of colour 1 the colour-1 residuals vanish: each such cell
+// was just solved exactly from its colour-0 neighbours) or of both colours;
+// the residual itself into rout when given, |f| max with fnorm.  Grid as
+// k_mg_sweep3; per-block maxima into part[b] (part[nb + b] for |f|).
+template <typename T, bool VARB>
+__global__ void __launch_bounds__(256, 4) k_mg_resid3(const __grid_constant__ MGOp<T> L,
+                                                      const T* __restrict__ x,
+                                                      const T* __restrict__ f,
+                                                      T* __restrict__ rout, int inhomog, int both,
+                                                      int fnorm, double* __restrict__ part)
+{
+    __shared__ double sh[32];
+    const int stop = L.stop ? *(volatile const int*)L.stop : 0;
+    const GridDev& g = L.g;
+    const int nx = g.n[0], nxh = nx >> 1, ny = g.n[1], nz = g.n[2];
+    const int ih = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int k0 = blockIdx.z * MG3_U;
+    const long long half = g.ncell() >> 1;
+    const bool active = ih < nxh && j < ny;
+    const bool edge = active && (j == 0 || j == ny - 1 || k0 == 0 || k0 + MG3_U > nz - 1);
+    const bool fastw = !__any_sync(0xffffffffu, edge);
+    double m = 0.0, mf = 0.0;
+    for (int col = 0; col < (both ? 2 : 1); ++col)
+    {
+        const T* xs = x + col * half;
+        const T* xo = x + (1 - col) * half;
+        const T* fc = f + col * half;
+        if (fastw && !active) continue;
+        if (fastw)
+        {
+            const int plane = nxh * ny;
+            const int hb = ih + nxh * (j + ny * k0);
+            T v[MG3_U][8];
+#pragma unroll
+            for (int u = 0; u < MG3_U; ++u)
+            {
+                const int q = (j + k0 + u + col) & 1;
+                const int h = hb + u * plane;
+                const int i = 2 * ih + q;
+                const int xlo = i == 0, xhi = i == nx - 1;
+                v[u][0] = __ldg(xo + (h + q - 1 + xlo));
+                v[u][1] = __ldg(xo + (h + q - xhi));
+                v[u][2] = __ldg(xo + (h - nxh));
+                v[u][3] = __ldg(xo + (h + nxh));
+                v[u][4] = __ldg(xo + (h - plane));
+                v[u][5] = __ldg(xo + (h + plane));
+                v[u][6] = __ldg(xs + h);
+                v[u][7] = __ldg(fc + h);
+            }
+#pragma unroll
+            for (int u = 0; u < MG3_U; ++u)
+            {
+                const int q = (j + k0 + u + col) & 1;
+                const int i = 2 * ih + q;
+                const int xo_ = (i == 0) ? 1 : ((i == nx - 1) ? 2 : 0);
+                T b[6];
+                mg3_faces<T, VARB>(L, i, j, k0 + u, b);
+                const T r = mg3_residual(L, v[u][7], v[u][6], v[u], b, xo_, i, j, k0 + u,
+                                         inhomog != 0);
+                if (rout && !stop) rout[col * half + hb + u * plane] = r;
+                const double a = fabs((double)r);
+                m = a > m ? a : m;
+                if (fnorm)
+                {
+                    const double af = fabs((double)v[u][7]);
+                    mf = af > mf ? af : mf;
+                }
+            }
+            continue;
+        }
+        if (!active) continue;
+        T v[MG3_U][8];
+        int outm[MG3_U];
+#pragma unroll
+        for (int u = 0; u < MG3_U; ++u)
+        {
+            const int k = min(k0 + u, nz - 1);
+            const int q = (j + k + col) & 1;
+            const int i = 2 * ih + q;
+            long long off[6];
+            outm[u] = mg3_offsets(g, i, j, k, q, off);
+            const long long h = ih + (long long)nxh * (j + (long long)ny * k);
+            v[u][6] = __ldg(xs + h);
+#pragma unroll
+            for (int d = 0; d < 6; ++d) v[u][d] = __ldg(xo + h + off[d]);
+            v[u][7] = __ldg(fc + h);
+        }
+#pragma unroll
+        for (int u = 0; u < MG3_U; ++u)
+        {
+            const int k = k0 + u;
+            if (k >= nz) break;
+            const int q = (j + k + col) & 1;
+            const int i = 2 * ih + q;
+            T b[6];
+            mg3_faces<T, VARB>(L, i, j, k, b);
+            const T r =
+                mg3_residual(L, v[u][7], v[u][6], v[u], b, outm[u], i, j, k, inhomog != 0);
+            if (rout && !stop) rout[col * half + ih + (long long)nxh * (j + (long long)ny * k)] = r;
+            const double a = fabs((double)r);
+            m = a > m ? a : m;
+            if (fnorm)
+            {
+                const double af = fabs((double)v[u][7]);
+                mf = af > mf ? af : mf;
+            }
+        }
+    }
+    m = block_max(m, sh);
+    if (fnorm) mf = block_max(mf, sh);
+    if (threadIdx.x == 0)
+    {
+        const long long nb = (long long)gridDim.x * gridDim.y * gridDim.z;
+        const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+        part[b] = m;
+        if (fnorm) part[nb + b] = mf;
+    }
+}
+
 // L(x) at an interior cell of a red-black split level, neighbours addressed
 // directly in the two colour halves (same arithmetic as mg_apply).
 template <typename T>
