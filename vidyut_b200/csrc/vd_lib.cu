@@ -371,6 +371,13 @@ void bottom(Hier<T>& H, const MGOp<T>& op, T* x, const T* f, cudaStream_t st)
            H.nub, H.nuf, H.status);
 }
 
+// Levels of at most this many cells run inside the one-CTA coarse cycle;
+// larger ones use the grid-wide kernels (a CTA sweeps ~2K cells per
+// microsecond, a kernel launch costs a few microseconds).
+#ifndef VD_MG_ONCHIP_CELLS
+#define VD_MG_ONCHIP_CELLS 4096
+#endif
+
 // One V-cycle on level-0 unknown x0 with right-hand side f0; the level-0
 // boundary data is inhomogeneous when `inh0` (the solution itself is
 // smoothed), homogeneous otherwise (a correction is smoothed).
@@ -390,7 +397,7 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
     }
     // first level small enough for the one-CTA coarse cycle (never level 0)
     int lc = L - 1;
-    while (lc > 1 && H.g[lc - 1].ncell() <= 4096) --lc;
+    while (lc > 1 && H.g[lc - 1].ncell() <= VD_MG_ONCHIP_CELLS) --lc;
     for (int l = 0; l < lc; ++l)
     {
         T* xl = l ? H.x[l] : x0;
@@ -428,10 +435,29 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         }
         // levels on chip when they fit (vd_create raises the kernel's dynamic
         // shared-memory limit to VD_MG_COARSE_SMEM)
-        const size_t smem = mg_coarse_smem(C);
-        const int on_chip = smem <= VD_MG_COARSE_SMEM ? 1 : 0;
-        k_mg_coarse_vcycle<T><<<1, 512, on_chip ? smem : 0, st>>>(
-            C, H.scratch, T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf, on_chip);
+        bool c3 = true; // all coarse levels 3-D, non-periodic, on chip
+        for (int l = lc; l < L; ++l)
+        {
+            const GridDev& g = H.g[l];
+            c3 = c3 && g.dim == 3 && !g.per[0] && !g.per[1] && !g.per[2] && !H.op[l].a &&
+                 g.n[0] < 1024 && g.n[1] < 1024 && g.n[2] < 1024;
+        }
+        const size_t smem3 = mg_coarse3_smem(C);
+        if (c3 && smem3 <= VD_MG_COARSE_SMEM)
+        {
+            if (H.varb)
+                k_mg_coarse3<T, true><<<1, MGC_THREADS, smem3, st>>>(
+                    C, T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf);
+            else
+                k_mg_coarse3<T, false><<<1, MGC_THREADS, smem3, st>>>(
+                    C, T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf);
+        } else
+        {
+            const size_t smem = mg_coarse_smem(C);
+            const int on_chip = smem <= VD_MG_COARSE_SMEM ? 1 : 0;
+            k_mg_coarse_vcycle<T><<<1, 512, on_chip ? smem : 0, st>>>(
+                C, H.scratch, T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf, on_chip);
+        }
         ++vd::g_launches;
         VD_CUDA_OK(cudaGetLastError());
     }
@@ -1503,6 +1529,12 @@ vd_status vd_create(const vd_config* cfg, void** out)
             h->nu1 = cfg->linsolve_num_pre_smooth;
             h->nu2 = cfg->linsolve_num_post_smooth;
         }
+        for (const void* kf : {(const void*)k_mg_coarse3<double, false>,
+                               (const void*)k_mg_coarse3<double, true>,
+                               (const void*)k_mg_coarse3<float, false>,
+                               (const void*)k_mg_coarse3<float, true>})
+            VD_CUDA_OK(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            VD_MG_COARSE_SMEM));
         VD_CUDA_OK(cudaFuncSetAttribute(k_mg_coarse_vcycle<double>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         VD_MG_COARSE_SMEM));

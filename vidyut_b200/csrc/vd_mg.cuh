@@ -1579,6 +1579,225 @@ __global__ void __launch_bounds__(512) k_mg_coarse_vcycle(MGCoarse<T> C, T* __re
     }
 }
 
+// ---------------------------------------------------------------------
+// The coarse end of a V-cycle on 3-D levels without periodic directions,
+// one 1024-thread CTA, every level on chip in natural layout.  Per cell
+// the operator is kept in the form the Gauss-Seidel update and the
+// residual both use:
+//     L x = G x0 - sum_n w_n x_n,   G = gamma - delta
+// where an outside neighbour n (homogeneous ghost c0 x0 + c1 x1) moves its
+// c0 share into G (delta) and its c1 share onto the opposite neighbour's
+// weight (the same operator as mg_apply / mg_gs_cell, rearranged).  G and
+// 1/G are formed once per launch; cell coordinates are decoded once.
+
+#define MGC_THREADS 1024
+
+template <typename T>
+struct MGCLevel
+{
+    T* x;
+    T* f;
+    T* G;
+    T* iG;
+    int* crd; // i | j << 10 | k << 20
+};
+
+// Per-side weights of cell (i,j,k): w[s2] for the neighbour on side s2
+// (x-lo, x-hi, y-lo, y-hi, z-lo, z-hi), the index offsets o[s2] (an outside
+// neighbour points at the opposite one, weight 0) and G.
+template <typename T, bool VARB>
+__device__ __forceinline__ void mgc_weights(const MGOp<T>& L, int i, int j, int k, T* w,
+                                            int* o, T& G)
+{
+    const int nx = L.g.n[0], ny = L.g.n[1], nz = L.g.n[2];
+    T b[6];
+    mg3_faces<T, VARB>(L, i, j, k, b);
+    const int st[3] = {1, nx, nx * ny};
+    const int c[3] = {i, j, k}, n[3] = {nx, ny, nz};
+    G = L.aconst;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+        const T dh = L.dh[d];
+        G += dh * (b[2 * d] + b[2 * d + 1]);
+        w[2 * d] = dh * b[2 * d];
+        w[2 * d + 1] = dh * b[2 * d + 1];
+        o[2 * d] = -st[d];
+        o[2 * d + 1] = st[d];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int hi = 0; hi < 2; ++hi)
+        {
+            const bool outside = hi ? (c[d] == n[d] - 1) : (c[d] == 0);
+            if (!outside) continue;
+            const int s2 = 2 * d + hi, s = d + 3 * hi;
+            const int p = (d == 0) ? (j + ny * k) : ((d == 1) ? (i + nx * k) : (i + nx * j));
+            const T c0 = L.c0[s] ? L.c0[s][p] : L.c0s[s];
+            const T c1 = L.c1s[s];
+            G -= w[s2] * c0;
+            w[s2 ^ 1] += w[s2] * c1;
+            w[s2] = T(0);
+            o[s2] = o[s2 ^ 1];
+        }
+}
+
+template <typename T, bool VARB>
+__device__ __forceinline__ T mgc_sum(const MGOp<T>& L, const T* __restrict__ x, int c, int i,
+                                     int j, int k)
+{
+    T w[6], G;
+    int o[6];
+    mgc_weights<T, VARB>(L, i, j, k, w, o, G);
+    T s = T(0);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) s += w[m] * x[c + o[m]];
+    return s;
+}
+
+template <typename T, bool VARB>
+__device__ void mgc_smooth(const MGOp<T>& L, const MGCLevel<T>& V, int nsm)
+{
+    const int n = (int)L.g.ncell();
+    for (int sm = 0; sm < nsm; ++sm)
+        for (int color = 0; color < 2; ++color)
+        {
+            for (int c = threadIdx.x; c < n; c += MGC_THREADS)
+            {
+                const int cr = V.crd[c];
+                const int i = cr & 1023, j = (cr >> 10) & 1023, k = cr >> 20;
+                if (((i + j + k) & 1) != color) continue;
+                V.x[c] = (V.f[c] + mgc_sum<T, VARB>(L, V.x, c, i, j, k)) * V.iG[c];
+            }
+            __syncthreads();
+        }
+}
+
+template <typename T, bool VARB>
+__global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3(MGCoarse<T> C, T rel, int maxiter,
+                                                            int nu1, int nu2, int nub, int nuf)
+{
+    extern __shared__ __align__(16) unsigned char mgc_smem[];
+    __shared__ T sh[32];
+    if (mg_stopped(C.op[C.lc])) return;
+    const int lc = C.lc, last = C.nl - 1;
+    MGCLevel<T> V[VD_MG_MAXLEV];
+    // carve the levels: x, f, G, 1/G (T) then the coordinates (int)
+    T* p = reinterpret_cast<T*>(mgc_smem);
+    for (int l = lc; l <= last; ++l)
+    {
+        const int n = (int)C.op[l].g.ncell();
+        V[l].x = p;
+        V[l].f = p + n;
+        V[l].G = p + 2 * n;
+        V[l].iG = p + 3 * n;
+        p += 4 * n;
+    }
+    T* bscr = p;
+    p += 6 * C.op[last].g.ncell();
+    int* ip = reinterpret_cast<int*>(p);
+    for (int l = lc; l <= last; ++l)
+    {
+        V[l].crd = ip;
+        ip += C.op[l].g.ncell();
+    }
+    // coordinates, G and 1/G of every level; level lc's right-hand side
+    for (int l = lc; l <= last; ++l)
+    {
+        const MGOp<T>& L = C.op[l];
+        const int nx = L.g.n[0], ny = L.g.n[1], n = (int)L.g.ncell();
+        for (int c = threadIdx.x; c < n; c += MGC_THREADS)
+        {
+            const int i = c % nx, r = c / nx, j = r % ny, k = r / ny;
+            V[l].crd[c] = i | (j << 10) | (k << 20);
+            T w[6], G;
+            int o[6];
+            mgc_weights<T, VARB>(L, i, j, k, w, o, G);
+            V[l].G[c] = G;
+            V[l].iG[c] = T(1) / G;
+            if (l == lc)
+            {
+                V[l].f[c] = C.f[l][L.g.idx(i, j, k)];
+                V[l].x[c] = T(0);
+            }
+        }
+    }
+    __syncthreads();
+    // descend
+    for (int l = lc; l < last; ++l)
+    {
+        const MGOp<T>& L = C.op[l];
+        mgc_smooth<T, VARB>(L, V[l], nu1);
+        const GridDev& gc = C.op[l + 1].g;
+        const int nx = L.g.n[0], ny = L.g.n[1];
+        const int ncx = gc.n[0], ncy = gc.n[1], nc = (int)gc.ncell();
+        for (int cc = threadIdx.x; cc < nc; cc += MGC_THREADS)
+        {
+            const int I = cc % ncx, R = cc / ncx, J = R % ncy, K = R / ncy;
+            T s = T(0);
+            for (int kk = 0; kk < 2; ++kk)
+                for (int jj = 0; jj < 2; ++jj)
+                    for (int ii = 0; ii < 2; ++ii)
+                    {
+                        const int i = 2 * I + ii, j = 2 * J + jj, k = 2 * K + kk;
+                        const int c = i + nx * (j + ny * k);
+                        const T ax = V[l].G[c] * V[l].x[c] - mgc_sum<T, VARB>(L, V[l].x, c, i, j, k);
+                        s += V[l].f[c] - ax;
+                    }
+            V[l + 1].f[cc] = s * T(0.125);
+            V[l + 1].x[cc] = T(0);
+        }
+        __syncthreads();
+    }
+    // bottom: BiCGStab (+ smoothing) in natural layout
+    {
+        MGOp<T> Lb = C.op[last];
+        Lb.g.rb = 0;
+        mg_bottom_block(Lb, V[last].x, V[last].f, bscr, rel, maxiter, nub, nuf, (int*)nullptr,
+                        sh);
+    }
+    // ascend
+    for (int l = last - 1; l >= lc; --l)
+    {
+        const MGOp<T>& L = C.op[l];
+        const GridDev& gc = C.op[l + 1].g;
+        const int n = (int)L.g.ncell();
+        const int ncx = gc.n[0], ncy = gc.n[1];
+        for (int c = threadIdx.x; c < n; c += MGC_THREADS)
+        {
+            const int cr = V[l].crd[c];
+            const int i = cr & 1023, j = (cr >> 10) & 1023, k = cr >> 20;
+            V[l].x[c] += V[l + 1].x[(i >> 1) + ncx * ((j >> 1) + ncy * (k >> 1))];
+        }
+        __syncthreads();
+        mgc_smooth<T, VARB>(L, V[l], nu2);
+    }
+    {
+        const MGOp<T>& L = C.op[lc];
+        const int n = (int)L.g.ncell();
+        for (int c = threadIdx.x; c < n; c += MGC_THREADS)
+        {
+            const int cr = V[lc].crd[c];
+            C.x[lc][L.g.idx(cr & 1023, (cr >> 10) & 1023, cr >> 20)] = V[lc].x[c];
+        }
+    }
+}
+
+// Shared memory of k_mg_coarse3 for levels lc .. nl-1.
+template <typename T>
+size_t mg_coarse3_smem(const MGCoarse<T>& C)
+{
+    size_t nt = 0, nc = 0;
+    for (int l = C.lc; l < C.nl; ++l)
+    {
+        nt += 4 * (size_t)C.op[l].g.ncell();
+        nc += (size_t)C.op[l].g.ncell();
+    }
+    nt += 6 * (size_t)C.op[C.nl - 1].g.ncell();
+    return nt * sizeof(T) + nc * sizeof(int);
+}
+
 // Mean of the coincident fine faces onto a coarse face.
 template <typename T>
 __global__ void k_mg_avg_faces(GridDev gf, GridDev gc, int d, const T* __restrict__ bf,
