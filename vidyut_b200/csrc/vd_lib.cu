@@ -295,16 +295,23 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                 const dim3 grid = mg3_grid(op.g);
                 const bool pro = xc && s == 0 && color == 0;
                 const GridDev gcv = gc ? *gc : op.g;
-                if (!pro && op.g.n[0] % 4 == 0)
+                if (op.g.n[0] % 4 == 0)
                 {
                     // pairs of half-cells per thread, 16-byte accesses
                     const dim3 gv((op.g.n[0] / 2 + 63) / 64, grid.y, grid.z);
-                    if (op.b[0])
-                        LAUNCH((k_mg_sweep3v<T, true>), gv, 256, st, op, x, f, color,
-                               inh ? 1 : 0, T(0));
+                    const T ig = op.b[0] ? T(0) : T(1) / gamma;
+                    if (op.b[0] && pro)
+                        LAUNCH((k_mg_sweep3v<T, true, true>), gv, 256, st, op, x, f, color,
+                               inh ? 1 : 0, ig, gcv, xc);
+                    else if (op.b[0])
+                        LAUNCH((k_mg_sweep3v<T, true, false>), gv, 256, st, op, x, f, color,
+                               inh ? 1 : 0, ig, gcv, xc);
+                    else if (pro)
+                        LAUNCH((k_mg_sweep3v<T, false, true>), gv, 256, st, op, x, f, color,
+                               inh ? 1 : 0, ig, gcv, xc);
                     else
-                        LAUNCH((k_mg_sweep3v<T, false>), gv, 256, st, op, x, f, color,
-                               inh ? 1 : 0, T(1) / gamma);
+                        LAUNCH((k_mg_sweep3v<T, false, false>), gv, 256, st, op, x, f, color,
+                               inh ? 1 : 0, ig, gcv, xc);
                 } else if (op.b[0])
                 {
                     if (pro)
@@ -468,8 +475,18 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         const bool inh = (l == 0) && inh0;
         if (mg3_ok(H.op[l]) && H.nu2 >= 1)
         {
-            smooth(H.op[l], xl, fl, inh, H.nu2, st, l == 0 ? H.prof_tag : VD_PROF_NONE,
-                   &H.g[l + 1], (const T*)H.x[l + 1]);
+            if (H.g[l].n[0] % 4 == 0)
+            {
+                // correction on colour 1 only; the first sweep (colour 0)
+                // rewrites colour 0 without reading it
+                const dim3 grid = mg3_grid(H.g[l]);
+                const dim3 gv((H.g[l].n[0] / 2 + 63) / 64, grid.y, grid.z);
+                LAUNCH(k_mg_prolong_c1<T>, gv, 256, st, H.g[l], H.g[l + 1], xl,
+                       (const T*)H.x[l + 1], H.op[l].stop);
+                smooth(H.op[l], xl, fl, inh, H.nu2, st, l == 0 ? H.prof_tag : VD_PROF_NONE);
+            } else
+                smooth(H.op[l], xl, fl, inh, H.nu2, st, l == 0 ? H.prof_tag : VD_PROF_NONE,
+                       &H.g[l + 1], (const T*)H.x[l + 1]);
             continue;
         }
         const Grid3 gp = rows3(H.g[l]);

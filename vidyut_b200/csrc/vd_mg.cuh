@@ -705,11 +705,12 @@ __device__ __forceinline__ T mg3_gs_value(const MGOp<T>& L, int i, int j, int k,
 // rows start 16-byte aligned).  Blocks of 32 pairs by 8 rows, MG3_U planes
 // per thread; warps with a row or plane on the level boundary update their
 // cells one by one with the ghost closure.
-template <typename T, bool VARB>
+template <typename T, bool VARB, bool PROL>
 __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ MGOp<T> L,
                                                        T* __restrict__ x,
                                                        const T* __restrict__ f, int color,
-                                                       int inhomog, T inv_gamma)
+                                                       int inhomog, T inv_gamma, GridDev gc,
+                                                       const T* __restrict__ xc)
 {
     using V2 = typename Vec2<T>::type;
     const int stop = L.stop ? *(volatile const int*)L.stop : 0;
@@ -748,12 +749,66 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
             vzp[u] = __ldg(reinterpret_cast<const V2*>(xo + h + plane));
             vf[u] = __ldg(reinterpret_cast<const V2*>(fs + h));
         }
+        // prolongation on the fly: an other-colour neighbour at half-index
+        // h' of row j has coarse column h'; cells A, B (coarse columns 2pr,
+        // 2pr+1) share their y and z neighbours' coarse rows and planes
+        T cxv[MG3_U][3], cyz[MG3_U][8];
+        if (PROL)
+        {
+#pragma unroll
+            for (int u = 0; u < MG3_U; ++u)
+            {
+                const int k = k0 + u;
+                const int q = (j + k + color) & 1;
+                const int J = j >> 1, K = k >> 1;
+#pragma unroll
+                for (int e = 0; e < 3; ++e)
+                {
+                    const int I = min(max(2 * pr - 1 + q + e, 0), nxh - 1);
+                    cxv[u][e] = __ldg(xc + gc.idx(I, J, K));
+                }
+                const int Jm = (j - 1) >> 1, Jp = (j + 1) >> 1, Km = (k - 1) >> 1,
+                          Kp = (k + 1) >> 1;
+#pragma unroll
+                for (int e = 0; e < 2; ++e)
+                {
+                    const int I = 2 * pr + e;
+                    cyz[u][e] = __ldg(xc + gc.idx(I, Jm, K));
+                    cyz[u][2 + e] = __ldg(xc + gc.idx(I, Jp, K));
+                    cyz[u][4 + e] = __ldg(xc + gc.idx(I, J, Km));
+                    cyz[u][6 + e] = __ldg(xc + gc.idx(I, J, Kp));
+                }
+            }
+        }
 #pragma unroll
         for (int u = 0; u < MG3_U; ++u)
         {
             const int k = k0 + u;
             const int q = (j + k + color) & 1;
             const int iA = 4 * pr + q, iB = iA + 2;
+            if (PROL)
+            {
+                // half-indices 2pr-1+q .. 2pr+1+q of the other colour
+                if (q == 0)
+                {
+                    sx[u] += cxv[u][0];
+                    vx[u].x += cxv[u][1];
+                    vx[u].y += cxv[u][2];
+                } else
+                {
+                    vx[u].x += cxv[u][0];
+                    vx[u].y += cxv[u][1];
+                    sx[u] += cxv[u][2];
+                }
+                vym[u].x += cyz[u][0];
+                vym[u].y += cyz[u][1];
+                vyp[u].x += cyz[u][2];
+                vyp[u].y += cyz[u][3];
+                vzm[u].x += cyz[u][4];
+                vzm[u].y += cyz[u][5];
+                vzp[u].x += cyz[u][6];
+                vzp[u].y += cyz[u][7];
+            }
             T nA[6], nB[6];
             if (q == 0)
             {
@@ -802,10 +857,52 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
             T nb[6];
 #pragma unroll
             for (int m = 0; m < 6; ++m) nb[m] = __ldg(xo + h + off[m]);
+            if (PROL)
+            {
+                const int ci[6] = {i - 1, i + 1, i, i, i, i}, cj[6] = {j, j, j - 1, j + 1, j, j},
+                          ck[6] = {k, k, k, k, k - 1, k + 1};
+#pragma unroll
+                for (int m = 0; m < 6; ++m)
+                {
+                    const int mm = (out & (1 << m)) ? (m ^ 1) : m;
+                    nb[m] += __ldg(xc + gc.idx(ci[mm] >> 1, cj[mm] >> 1, ck[mm] >> 1));
+                }
+            }
             const T v = mg3_gs_value<T, VARB>(L, i, j, k, out, inhomog != 0, inv_gamma,
                                               __ldg(fs + h), nb);
             if (!stop) xs[h] = v;
         }
+    }
+}
+
+// Prolongation for the post-smoothing: x += P e on the colour-1 cells only
+// (the colour-0 cells are rewritten by the first sweep, colour 0, which
+// does not read their previous values).  Pairs of half-cells per thread
+// (nx % 4 == 0); colour-1 cells 4pr+q1 and 4pr+2+q1 of row j have coarse
+// columns 2pr and 2pr+1.  Grid as k_mg_sweep3v.
+template <typename T>
+__global__ void __launch_bounds__(256) k_mg_prolong_c1(GridDev g, GridDev gc, T* __restrict__ x,
+                                                       const T* __restrict__ xc,
+                                                       const int* stop)
+{
+    using V2 = typename Vec2<T>::type;
+    if (stop && *(volatile const int*)stop) return;
+    const int nxh = g.n[0] >> 1, ny = g.n[1], nz = g.n[2];
+    const int pr = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int k0 = blockIdx.z * MG3_U;
+    if (2 * pr >= nxh || j >= ny) return;
+    T* __restrict__ x1 = x + (g.ncell() >> 1);
+#pragma unroll
+    for (int u = 0; u < MG3_U; ++u)
+    {
+        const int k = k0 + u;
+        if (k >= nz) break;
+        const long long h = 2 * pr + (long long)nxh * (j + (long long)ny * k);
+        V2 v = *reinterpret_cast<const V2*>(x1 + h);
+        v.x += __ldg(xc + gc.idx(2 * pr, j >> 1, k >> 1));
+        v.y += __ldg(xc + gc.idx(2 * pr + 1, j >> 1, k >> 1));
+        *reinterpret_cast<V2*>(x1 + h) = v;
     }
 }
 
