@@ -461,47 +461,47 @@ __global__ void __launch_bounds__(256, 2) k_explicit_stream(ExplParams P, int q0
                 }
             }
         __syncthreads();
-        // ---- x and y face fluxes of plane p
-        if (P.do_transport && active)
+        // ---- x and y face fluxes of plane p: the (EX_TX+1) x EX_TY x-faces and
+        // EX_TX x (EX_TY+1) y-faces of the tile spread evenly over the threads
+        if (P.do_transport)
         {
-#pragma unroll
-            for (int s = 0; s < EX_QB; ++s)
+            constexpr int NFX = (EX_TX + 1) * EX_TY, NFY = EX_TX * (EX_TY + 1);
+            const int nfy = (dim > 1) ? NFY : 0;
+            for (int fid = threadIdx.x; fid < NFX + nfy; fid += blockDim.x)
             {
-                if (s >= nq) break;
-                const int qc = q0 + s;
-                double u[7], v[7];
+                const bool xf = fid < NFX;
+                const int r = xf ? fid / (EX_TX + 1) : (fid - NFX) / EX_TX;
+                const int c = xf ? fid - r * (EX_TX + 1) : (fid - NFX) - r * EX_TX;
+                // face index along its direction, and whether it is needed
+                const int fi = i0 + c, fj = j0 + r;
+                const bool need = xf ? (fi <= g.n[0] && fi - 1 < g.n[0] && fj < g.n[1])
+                                     : (fj <= g.n[1] && fj - 1 < g.n[1] && fi < g.n[0]);
+                if (!need) continue;
 #pragma unroll
-                for (int m = 0; m < 7; ++m)
+                for (int s = 0; s < EX_QB; ++s)
                 {
-                    u[m] = s_n[s][ty + 3][tx + m];
-                    v[m] = s_vx[s][ty + 3][tx + m];
-                }
-                double f = face_flux6(u, v, P.hyp_order, P.weno_scheme, dxmin, P.dt);
-                if (i == 0 && wall_zero(P.bclo[qc][0])) f = 0.0;
-                s_fx[s][ty][tx] = f;
-                if (tx == EX_TX - 1 || i == g.n[0] - 1)
-                {
-                    double fh = face_flux6(u + 1, v + 1, P.hyp_order, P.weno_scheme, dxmin, P.dt);
-                    if (i == g.n[0] - 1 && wall_zero(P.bchi[qc][0])) fh = 0.0;
-                    s_fx[s][ty][tx + 1] = fh;
-                }
-                if (dim > 1)
-                {
+                    if (s >= nq) break;
+                    const int qc = q0 + s;
+                    double u[6], v[6];
 #pragma unroll
-                    for (int m = 0; m < 7; ++m)
+                    for (int m = 0; m < 6; ++m)
                     {
-                        u[m] = s_n[s][ty + m][tx + 3];
-                        v[m] = s_vy[s][ty + m][tx + 3];
+                        u[m] = xf ? s_n[s][r + 3][c + m] : s_n[s][r + m][c + 3];
+                        v[m] = xf ? s_vx[s][r + 3][c + m] : s_vy[s][r + m][c + 3];
                     }
-                    double fy = face_flux6(u, v, P.hyp_order, P.weno_scheme, dxmin, P.dt);
-                    if (j == 0 && wall_zero(P.bclo[qc][1])) fy = 0.0;
-                    s_fy[s][ty][tx] = fy;
-                    if (ty == EX_TY - 1 || j == g.n[1] - 1)
+                    double fl = face_flux6(u, v, P.hyp_order, P.weno_scheme, dxmin, P.dt);
+                    if (xf)
                     {
-                        double fh =
-                            face_flux6(u + 1, v + 1, P.hyp_order, P.weno_scheme, dxmin, P.dt);
-                        if (j == g.n[1] - 1 && wall_zero(P.bchi[qc][1])) fh = 0.0;
-                        s_fy[s][ty + 1][tx] = fh;
+                        if ((fi == 0 && wall_zero(P.bclo[qc][0])) ||
+                            (fi == g.n[0] && wall_zero(P.bchi[qc][0])))
+                            fl = 0.0;
+                        s_fx[s][r][c] = fl;
+                    } else
+                    {
+                        if ((fj == 0 && wall_zero(P.bclo[qc][1])) ||
+                            (fj == g.n[1] && wall_zero(P.bchi[qc][1])))
+                            fl = 0.0;
+                        s_fy[s][r][c] = fl;
                     }
                 }
             }
