@@ -616,7 +616,8 @@ double read_norm(Ctx& c)
 // the bit patterns at mx[0] (|r|) and mx[1] (|f| when `fnorm`).
 template <typename T>
 void launch_norm(Ctx& c, const MGOp<T>& op, const T* x, const T* f, T* rout, bool inh,
-                 bool fnorm, unsigned long long* mx, bool both = true)
+                 bool fnorm, unsigned long long* mx, bool both = true, float* r32 = nullptr,
+                 float* x32 = nullptr, const double* rscale = nullptr)
 {
     if (mg3_ok(op))
     {
@@ -626,10 +627,10 @@ void launch_norm(Ctx& c, const MGOp<T>& op, const T* x, const T* f, T* rout, boo
         {
             if (op.b[0])
                 LAUNCH((k_mg_resid3<T, true>), grid, 256, c.st, op, x, f, rout, inh ? 1 : 0,
-                       both ? 1 : 0, fnorm ? 1 : 0, c.dpart);
+                       both ? 1 : 0, fnorm ? 1 : 0, c.dpart, r32, x32, rscale);
             else
                 LAUNCH((k_mg_resid3<T, false>), grid, 256, c.st, op, x, f, rout, inh ? 1 : 0,
-                       both ? 1 : 0, fnorm ? 1 : 0, c.dpart);
+                       both ? 1 : 0, fnorm ? 1 : 0, c.dpart, r32, x32, rscale);
             LAUNCH(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nb, fnorm ? 1 : 0, mx);
             return;
         }
@@ -719,7 +720,7 @@ void bind_sides32(Ctx& c, Hier<float>& H, SideArrays* sides, const int* bct)
 // solution.  Refined: FP64 residual, FP32 V-cycles on the normalised
 // correction, FP64 update; both stop on |r|_inf <= max(abs, rel |r0|_inf).
 int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* rhs,
-             vd_solve_stats* stats, int hint = 1)
+             vd_solve_stats* stats, int hint = 1, bool allow32 = true)
 {
     const vd_config& cfg = c.cfg;
     double b0 = 0.0;
@@ -734,7 +735,59 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
     if (r0 > target)
     {
         st.converged = 0;
-        if (cfg.mg_precision == VD_MG_FP32_REFINED)
+        const bool refined = cfg.mg_precision == VD_MG_FP32_REFINED && allow32;
+        if (refined && mg3_ok(H64.op[0]))
+        {
+            // device-side refinement: each pass is the FP64 residual written
+            // as the scaled FP32 right-hand side (with the FP32 unknown
+            // zeroed), a device convergence check, `inner` FP32 V-cycles and
+            // the FP64 update; passes are enqueued in batches and every
+            // kernel returns at once when the stop flag is up
+            const long long n = c.N;
+            const int inner = std::max(1, cfg.mg_inner_cycles);
+            MGDev init{};
+            init.sc_cur = 1.0 / r0;
+            VD_CUDA_OK(cudaMemcpyAsync(c.dmg, &init, sizeof(MGDev), cudaMemcpyHostToDevice, c.st));
+            MGOp<double> op0 = H64.op[0];
+            op0.stop = &c.dmg->done;
+            for (auto& o : H32.op) o.stop = &c.dmg->done;
+            int issued = 0;
+            int batch = std::max(1, (hint + inner - 1) / inner - 1);
+            while (issued * inner < cfg.linsolve_maxiter)
+            {
+                const int nb = std::min(batch, (cfg.linsolve_maxiter - issued * inner + inner - 1) / inner);
+                for (int b = 0; b < nb; ++b)
+                {
+                    launch_norm(c, op0, (const double*)sol, (const double*)rhs, (double*)nullptr,
+                                true, false, &c.dmg->rbits, true, H32.f[0], H32.x[0],
+                                &c.dmg->sc_cur);
+                    LAUNCH(k_ref_check, 1, 1, c.st, c.dmg, target);
+                    for (int q = 0; q < inner; ++q) vcycle(H32, H32.x[0], H32.f[0], false, c.dscal, c.st);
+                    LAUNCH(k_ref_add, gsz(n), BS, c.st, sol, (const float*)H32.x[0],
+                           (const MGDev*)c.dmg, n);
+                    LAUNCH(k_ref_rotate, 1, 1, c.st, c.dmg, inner);
+                    ++issued;
+                }
+                VD_CUDA_OK(cudaMemcpyAsync(c.hmg, c.dmg, sizeof(MGDev), cudaMemcpyDeviceToHost, c.st));
+                VD_CUDA_OK(cudaStreamSynchronize(c.st));
+                if (c.hmg->done) break;
+                batch = 2;
+            }
+            if (!c.hmg->done)
+            {
+                // the last pass's update has no residual check yet: take it
+                launch_norm(c, op0, (const double*)sol, (const double*)rhs, (double*)nullptr,
+                            true, false, &c.dmg->rbits, true, H32.f[0], H32.x[0], &c.dmg->sc_cur);
+                LAUNCH(k_ref_check, 1, 1, c.st, c.dmg, target);
+                VD_CUDA_OK(cudaMemcpyAsync(c.hmg, c.dmg, sizeof(MGDev), cudaMemcpyDeviceToHost, c.st));
+                VD_CUDA_OK(cudaStreamSynchronize(c.st));
+            }
+            for (auto& o : H32.op) o.stop = nullptr;
+            st.iterations = c.hmg->iters;
+            st.refinements = c.hmg->refs;
+            std::memcpy(&st.final_residual, &c.hmg->final_bits, sizeof(double));
+            st.converged = c.hmg->done;
+        } else if (refined)
         {
             const long long n = c.N;
             double rn = r0;
@@ -940,7 +993,11 @@ void species_solve(Ctx& c, int comp, double time, const double* Sold, vd_solve_s
                    (const double*)c.HS.bf[0][s % 3], 1.0, ts, c.G.dx[s % 3], c.sside[s].val,
                    c.spec_rhs);
     vd_solve_stats st{};
-    const int it = mg_solve(c, c.HS, c.HS32, c.u[comp], c.spec_rhs, &st, c.hint[comp]);
+    // a species solve that took one or two V-cycles last time (the strongly
+    // diagonal implicit-diffusion operator) runs them in FP64: a refinement
+    // pass costs more than the cycle it would save
+    const bool allow32 = c.hint[comp] == 0 || c.hint[comp] > 2;
+    const int it = mg_solve(c, c.HS, c.HS32, c.u[comp], c.spec_rhs, &st, c.hint[comp], allow32);
     if (st.converged && it > 0) c.hint[comp] = it;
     c.species_iters += it;
     if (stats) *stats = st;

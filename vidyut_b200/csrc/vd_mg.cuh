@@ -487,7 +487,9 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3(const __grid_constant__ MG
                                                       int inhomog, T inv_gamma, GridDev gc,
                                                       const T* __restrict__ xc)
 {
-    const int stop = L.stop ? *(volatile const int*)L.stop : 0;
+    // the stop flag only changes between kernels: a read-only (cached) load
+    const int stop = L.stop ? __ldg(L.stop) : 0;
+    if (stop) return;
     const GridDev& g = L.g;
     const int nx = g.n[0], nxh = nx >> 1, ny = g.n[1], nz = g.n[2];
     const int ih = blockIdx.x * 32 + (threadIdx.x & 31);
@@ -713,7 +715,9 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
                                                        const T* __restrict__ xc)
 {
     using V2 = typename Vec2<T>::type;
-    const int stop = L.stop ? *(volatile const int*)L.stop : 0;
+    // the stop flag only changes between kernels: a read-only (cached) load
+    const int stop = L.stop ? __ldg(L.stop) : 0;
+    if (stop) return;
     const GridDev& g = L.g;
     const int nx = g.n[0], nxh = nx >> 1, ny = g.n[1], nz = g.n[2];
     const int pr = blockIdx.x * 32 + (threadIdx.x & 31); // pair index: half-cells 2pr, 2pr+1
@@ -945,7 +949,9 @@ __global__ void __launch_bounds__(256, 3) k_mg_restrict3(const __grid_constant__
                                                       T* __restrict__ fc, T* __restrict__ xc,
                                                       int inhomog)
 {
-    const int stop = L.stop ? *(volatile const int*)L.stop : 0;
+    // the stop flag only changes between kernels: a read-only (cached) load
+    const int stop = L.stop ? __ldg(L.stop) : 0;
+    if (stop) return;
     const GridDev& g = L.g;
     const int nxh = g.n[0] >> 1, ny = g.n[1];
     const int I = blockIdx.x * 32 + (threadIdx.x & 31);
@@ -1059,10 +1065,15 @@ __global__ void __launch_bounds__(256, 4) k_mg_resid3(const __grid_constant__ MG
                                                       const T* __restrict__ x,
                                                       const T* __restrict__ f,
                                                       T* __restrict__ rout, int inhomog, int both,
-                                                      int fnorm, double* __restrict__ part)
+                                                      int fnorm, double* __restrict__ part,
+                                                      float* __restrict__ r32 = nullptr,
+                                                      float* __restrict__ x32 = nullptr,
+                                                      const double* rscale = nullptr)
 {
     __shared__ double sh[32];
-    const int stop = L.stop ? *(volatile const int*)L.stop : 0;
+    // the stop flag only changes between kernels: a read-only (cached) load
+    const int stop = L.stop ? __ldg(L.stop) : 0;
+    if (stop) return;
     const GridDev& g = L.g;
     const int nx = g.n[0], nxh = nx >> 1, ny = g.n[1], nz = g.n[2];
     const int ih = blockIdx.x * 32 + (threadIdx.x & 31);
@@ -1072,6 +1083,8 @@ __global__ void __launch_bounds__(256, 4) k_mg_resid3(const __grid_constant__ MG
     const bool active = ih < nxh && j < ny;
     const bool edge = active && (j == 0 || j == ny - 1 || k0 == 0 || k0 + MG3_U > nz - 1);
     const bool fastw = !__any_sync(0xffffffffu, edge);
+    // refinement form: r32 = r * rscale (the previous residual's 1/max), x32 = 0
+    const double rs = r32 ? *rscale : 0.0;
     double m = 0.0, mf = 0.0;
     for (int col = 0; col < (both ? 2 : 1); ++col)
     {
@@ -1111,6 +1124,11 @@ __global__ void __launch_bounds__(256, 4) k_mg_resid3(const __grid_constant__ MG
                 const T r = mg3_residual(L, v[u][7], v[u][6], v[u], b, xo_, i, j, k0 + u,
                                          inhomog != 0);
                 if (rout && !stop) rout[col * half + hb + u * plane] = r;
+                if (r32 && !stop)
+                {
+                    r32[col * half + hb + u * plane] = (float)((double)r * rs);
+                    x32[col * half + hb + u * plane] = 0.0f;
+                }
                 const double a = fabs((double)r);
                 m = a > m ? a : m;
                 if (fnorm)
@@ -1150,6 +1168,12 @@ __global__ void __launch_bounds__(256, 4) k_mg_resid3(const __grid_constant__ MG
             const T r =
                 mg3_residual(L, v[u][7], v[u][6], v[u], b, outm[u], i, j, k, inhomog != 0);
             if (rout && !stop) rout[col * half + ih + (long long)nxh * (j + (long long)ny * k)] = r;
+            if (r32 && !stop)
+            {
+                const long long o = col * half + ih + (long long)nxh * (j + (long long)ny * k);
+                r32[o] = (float)((double)r * rs);
+                x32[o] = 0.0f;
+            }
             const double a = fabs((double)r);
             m = a > m ? a : m;
             if (fnorm)
@@ -1987,6 +2011,9 @@ struct MGDev
     unsigned long long final_bits; // residual after the last counted cycle
     int done;
     int iters;
+    int refs;       // refinement passes of the FP32-refined form
+    double sc_cur;  // scale of the FP32 right-hand side being solved for
+    double sc_next; // 1 / max-norm of the latest residual
 };
 
 // After each V-cycle: count it and raise the stop flag once the residual
@@ -1997,5 +2024,39 @@ __global__ void k_mg_check(MGDev* s, double target)
     s->iters += 1;
     s->final_bits = s->rbits;
     if (__longlong_as_double((long long)s->rbits) <= target) s->done = 1;
+}
+
+// FP32-refined form, on the device: after the FP64 residual of the current
+// solution, stop once it meets the target, else keep its 1/max-norm as the
+// next right-hand side scale.
+__global__ void k_ref_check(MGDev* s, double target)
+{
+    if (s->done) return;
+    s->final_bits = s->rbits;
+    const double r = __longlong_as_double((long long)s->rbits);
+    if (r <= target)
+        s->done = 1;
+    else
+        s->sc_next = 1.0 / r;
+}
+
+// x += e / sc_cur (the correction of the scaled FP32 equation).
+__global__ void k_ref_add(double* __restrict__ x, const float* __restrict__ e, const MGDev* s,
+                          long long n)
+{
+    if (*(volatile const int*)&s->done) return;
+    const double inv = 1.0 / s->sc_cur;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        x[t] += (double)e[t] * inv;
+}
+
+// One refinement pass completed: count it and move to the next scale.
+__global__ void k_ref_rotate(MGDev* s, int inner)
+{
+    if (s->done) return;
+    s->refs += 1;
+    s->iters += inner;
+    s->sc_cur = s->sc_next;
 }
 } // namespace vd
