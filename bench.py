@@ -290,12 +290,15 @@ def main():
     avg_s = (pms / nl) / 1e3 if nl else float("nan")
     achieved = pbytes / avg_s / 1e9 if nl else None
     traffic = load_traffic()
-    roof = {"kernel": "k_mg_smooth_color<double> (Poisson fine level)", "bound": "hbm",
+    roof = {"kernel": "k_mg_sweep3v<double> (Poisson fine-level red-black colour sweep, "
+                      "12 B/cell: other colour of x, this colour of f, write this colour)",
+            "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
             "algorithmic_bytes_per_launch": pbytes, "launches_timed": nl,
             "avg_launch_us": avg_s * 1e6 if nl else None,
-            "traffic": (traffic or {}).get("bytes_per_launch") if traffic else None}
+            "traffic": (traffic or {}).get("bytes_per_launch") if traffic else None,
+            "traffic_note": (traffic or {}).get("note") if traffic else None}
 
     if args.lean:
         if rank == 0:

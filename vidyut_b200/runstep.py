@@ -1,0 +1,57 @@
+"""Run the benchmark workload for an external profiler (ncu and the like).
+
+    python -m vidyut_b200.runstep [--n 256] [--warmup 3] [--steps 1] [--fp32]
+    python -m vidyut_b200.runstep --n 208 --solve           # one field solve
+    python -m vidyut_b200.runstep --n 192 --solve --explicit  # + explicit sources
+
+The workload is the two-species Townsend discharge of ``bench.py``
+(``workloads.townsend_config(3, n)``, seeded initial state 0).  With
+``--steps`` the last line reports the launches and the device time of the
+timed steps, so a launch list can be cut to exactly those launches.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--fp32", action="store_true", help="FP32-refined multigrid form")
+    ap.add_argument("--solve", action="store_true", help="one field solve instead of steps")
+    ap.add_argument("--explicit", action="store_true", help="with --solve: explicit sources too")
+    a = ap.parse_args()
+
+    import vidyut_b200 as vb
+    from vidyut_b200 import workloads as W
+
+    cfg = W.townsend_config(3, a.n)
+    if a.fp32:
+        cfg["mg_precision"] = vb.VD_MG_FP32_REFINED
+    g = vb.Vidyut(cfg)
+    g.set_state(0, W.initial_state(cfg, 0))
+    if a.solve:
+        st = g.solve_potential(0.0)
+        if a.explicit:
+            g.explicit_rhs(0.0)
+        print(f"field solve: {st.iterations} V-cycles, converged {st.converged}")
+    else:
+        g.step(a.warmup)
+        l0 = g.launch_count()
+        st = g.step(a.steps)
+        print(f"timed steps {a.steps}: {g.launch_count() - l0} launches, "
+              f"{st.gpu_ms:.3f} ms device time, poisson V-cycles {st.poisson_iterations}, "
+              f"species V-cycles {st.species_iterations}")
+    g.close()
+
+
+if __name__ == "__main__":
+    main()
