@@ -623,6 +623,20 @@ void launch_norm(Ctx& c, const MGOp<T>& op, const T* x, const T* f, T* rout, boo
     {
         const dim3 grid = mg3_grid(op.g);
         const long long nb = (long long)grid.x * grid.y * grid.z;
+        const dim3 gv((op.g.n[0] / 2 + 63) / 64, grid.y, grid.z);
+        const long long nbv = (long long)gv.x * gv.y * gv.z;
+        if (op.g.n[0] % 4 == 0 && nbv <= c.npart)
+        {
+            // pairs of half-cells per thread, 16-byte accesses
+            if (op.b[0])
+                LAUNCH((k_mg_resid3v<T, true>), gv, 256, c.st, op, x, f, rout, inh ? 1 : 0,
+                       both ? 1 : 0, fnorm ? 1 : 0, c.dpart, r32, x32, rscale);
+            else
+                LAUNCH((k_mg_resid3v<T, false>), gv, 256, c.st, op, x, f, rout, inh ? 1 : 0,
+                       both ? 1 : 0, fnorm ? 1 : 0, c.dpart, r32, x32, rscale);
+            LAUNCH(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nbv, fnorm ? 1 : 0, mx);
+            return;
+        }
         if (nb <= c.npart)
         {
             if (op.b[0])

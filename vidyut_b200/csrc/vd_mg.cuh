@@ -1055,6 +1055,161 @@ __global__ void __launch_bounds__(256, 3) k_mg_restrict3(const __grid_constant__
     xc[pc] = T(0);
 }
 
+// The same residual max-norm with two adjacent half-cells per thread and
+// 16-byte accesses (nx % 4 == 0), as k_mg_sweep3v; outputs and arguments as
+// k_mg_resid3.  Blocks of 32 pairs by 8 rows, MG3_U planes per thread.
+template <typename T, bool VARB>
+__global__ void __launch_bounds__(256, 4) k_mg_resid3v(const __grid_constant__ MGOp<T> L,
+                                                       const T* __restrict__ x,
+                                                       const T* __restrict__ f,
+                                                       T* __restrict__ rout, int inhomog,
+                                                       int both, int fnorm,
+                                                       double* __restrict__ part,
+                                                       float* __restrict__ r32 = nullptr,
+                                                       float* __restrict__ x32 = nullptr,
+                                                       const double* rscale = nullptr)
+{
+    using V2 = typename Vec2<T>::type;
+    __shared__ double sh[32];
+    const int stop = L.stop ? __ldg(L.stop) : 0;
+    if (stop) return;
+    const GridDev& g = L.g;
+    const int nx = g.n[0], nxh = nx >> 1, ny = g.n[1], nz = g.n[2];
+    const int pr = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int k0 = blockIdx.z * MG3_U;
+    const bool active = 2 * pr < nxh && j < ny;
+    const long long half = g.ncell() >> 1;
+    const bool edge = active && (j == 0 || j == ny - 1 || k0 == 0 || k0 + MG3_U > nz - 1);
+    const bool fastw = !__any_sync(0xffffffffu, edge);
+    const double rs = r32 ? *rscale : 0.0;
+    double m = 0.0, mf = 0.0;
+    auto emit = [&](long long o, T r, T fv, bool wr) {
+        if (wr && rout) rout[o] = r;
+        if (r32)
+        {
+            r32[o] = (float)((double)r * rs);
+            x32[o] = 0.0f;
+        }
+        const double a = fabs((double)r);
+        m = a > m ? a : m;
+        if (fnorm)
+        {
+            const double af = fabs((double)fv);
+            mf = af > mf ? af : mf;
+        }
+    };
+    for (int col = 0; col < (both ? 2 : 1); ++col)
+    {
+        const T* xs = x + col * half;
+        const T* xo = x + (1 - col) * half;
+        const T* fc = f + col * half;
+        if (!active) continue;
+        if (fastw)
+        {
+            const int plane = nxh * ny;
+            const int hb = 2 * pr + nxh * (j + ny * k0);
+            V2 vx[MG3_U], vym[MG3_U], vyp[MG3_U], vzm[MG3_U], vzp[MG3_U], vf[MG3_U], v0[MG3_U];
+            T sx[MG3_U];
+#pragma unroll
+            for (int u = 0; u < MG3_U; ++u)
+            {
+                const int q = (j + k0 + u + col) & 1;
+                const int h = hb + u * plane;
+                const bool xlo = q == 0 && pr == 0, xhi = q == 1 && 2 * pr + 2 == nxh;
+                const int so = q ? (xhi ? 1 : 2) : (xlo ? 0 : -1);
+                v0[u] = __ldg(reinterpret_cast<const V2*>(xs + h));
+                vx[u] = __ldg(reinterpret_cast<const V2*>(xo + h));
+                sx[u] = __ldg(xo + h + so);
+                vym[u] = __ldg(reinterpret_cast<const V2*>(xo + h - nxh));
+                vyp[u] = __ldg(reinterpret_cast<const V2*>(xo + h + nxh));
+                vzm[u] = __ldg(reinterpret_cast<const V2*>(xo + h - plane));
+                vzp[u] = __ldg(reinterpret_cast<const V2*>(xo + h + plane));
+                vf[u] = __ldg(reinterpret_cast<const V2*>(fc + h));
+            }
+#pragma unroll
+            for (int u = 0; u < MG3_U; ++u)
+            {
+                const int k = k0 + u;
+                const int q = (j + k + col) & 1;
+                const int iA = 4 * pr + q, iB = iA + 2;
+                T nA[6], nB[6];
+                if (q == 0)
+                {
+                    nA[0] = sx[u];
+                    nA[1] = vx[u].x;
+                    nB[0] = vx[u].x;
+                    nB[1] = vx[u].y;
+                } else
+                {
+                    nA[0] = vx[u].x;
+                    nA[1] = vx[u].y;
+                    nB[0] = vx[u].y;
+                    nB[1] = sx[u];
+                }
+                nA[2] = vym[u].x;
+                nB[2] = vym[u].y;
+                nA[3] = vyp[u].x;
+                nB[3] = vyp[u].y;
+                nA[4] = vzm[u].x;
+                nB[4] = vzm[u].y;
+                nA[5] = vzp[u].x;
+                nB[5] = vzp[u].y;
+                T bA[6], bB[6];
+                mg3_faces<T, VARB>(L, iA, j, k, bA);
+                mg3_faces<T, VARB>(L, iB, j, k, bB);
+                const int oA = (iA == 0) ? 1 : 0, oB = (iB == nx - 1) ? 2 : 0;
+                const T rA = mg3_residual(L, vf[u].x, v0[u].x, nA, bA, oA, iA, j, k, inhomog != 0);
+                const T rB = mg3_residual(L, vf[u].y, v0[u].y, nB, bB, oB, iB, j, k, inhomog != 0);
+                const long long o = col * half + hb + u * plane;
+                if (rout)
+                {
+                    V2 w;
+                    w.x = rA;
+                    w.y = rB;
+                    *reinterpret_cast<V2*>(rout + o) = w;
+                }
+                emit(o, rA, vf[u].x, false);
+                emit(o + 1, rB, vf[u].y, false);
+            }
+            continue;
+        }
+        // boundary rows and planes: cell by cell
+#pragma unroll 1
+        for (int u = 0; u < MG3_U; ++u)
+        {
+            const int k = k0 + u;
+            if (k >= nz) break;
+            for (int e = 0; e < 2; ++e)
+            {
+                const int ih = 2 * pr + e;
+                const int q = (j + k + col) & 1;
+                const int i = 2 * ih + q;
+                long long off[6];
+                const int out = mg3_offsets(g, i, j, k, q, off);
+                const long long h = ih + (long long)nxh * (j + (long long)ny * k);
+                T nb[6];
+#pragma unroll
+                for (int d = 0; d < 6; ++d) nb[d] = __ldg(xo + h + off[d]);
+                T b[6];
+                mg3_faces<T, VARB>(L, i, j, k, b);
+                const T fv = __ldg(fc + h);
+                const T r = mg3_residual(L, fv, __ldg(xs + h), nb, b, out, i, j, k, inhomog != 0);
+                emit(col * half + h, r, fv, true);
+            }
+        }
+    }
+    m = block_max(m, sh);
+    if (fnorm) mf = block_max(mf, sh);
+    if (threadIdx.x == 0)
+    {
+        const long long nb = (long long)gridDim.x * gridDim.y * gridDim.z;
+        const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+        part[b] = m;
+        if (fnorm) part[nb + b] = mf;
+    }
+}
+
 // Residual max-norm on a 3-D red-black split level: cells of colour 0 only
 // (after a sweep of colour 1 the colour-1 residuals vanish: each such cell
 // was just solved exactly from its colour-0 neighbours) or of both colours;
