@@ -391,7 +391,13 @@ __device__ __forceinline__ void ex_cell_vel(const ExplParams& P, int ci, int cj,
     vz = mu * ez;
 }
 
-__global__ void __launch_bounds__(256, 2) k_explicit_stream(ExplParams P, int q0, int zc)
+#ifndef EX_ZC
+#define EX_ZC 32 // planes per CTA in z (+ 6 halo planes of the z stencil)
+#endif
+#ifndef EX_MINB
+#define EX_MINB 3 // CTAs per SM the register budget is sized for (measured: 3 beats 2)
+#endif
+__global__ void __launch_bounds__(256, EX_MINB) k_explicit_stream(ExplParams P, int q0, int zc)
 {
     __shared__ double s_n[EX_QB][EX_HY][EX_HX];
     __shared__ double s_vx[EX_QB][EX_HY][EX_HX];

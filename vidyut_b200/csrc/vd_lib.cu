@@ -298,20 +298,21 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                 if (op.g.n[0] % 4 == 0)
                 {
                     // pairs of half-cells per thread, 16-byte accesses
-                    const dim3 gv((op.g.n[0] / 2 + 63) / 64, grid.y, grid.z);
+                    const bool two = op.g.ncell() >= (8LL << 20); // planes per thread
+                    const int uv = two ? 2 : 1;
+                    const dim3 gv((op.g.n[0] / 2 + 63) / 64, grid.y, (op.g.n[2] + uv - 1) / uv);
                     const T ig = op.b[0] ? T(0) : T(1) / gamma;
+#define VD_SWEEP3V(VB, PR, UV)                                                                \
+    LAUNCH((k_mg_sweep3v<T, VB, PR, UV>), gv, 256, st, op, x, f, color, inh ? 1 : 0, ig, gcv, xc)
                     if (op.b[0] && pro)
-                        LAUNCH((k_mg_sweep3v<T, true, true>), gv, 256, st, op, x, f, color,
-                               inh ? 1 : 0, ig, gcv, xc);
+                        { if (two) VD_SWEEP3V(true, true, 2); else VD_SWEEP3V(true, true, 1); }
                     else if (op.b[0])
-                        LAUNCH((k_mg_sweep3v<T, true, false>), gv, 256, st, op, x, f, color,
-                               inh ? 1 : 0, ig, gcv, xc);
+                        { if (two) VD_SWEEP3V(true, false, 2); else VD_SWEEP3V(true, false, 1); }
                     else if (pro)
-                        LAUNCH((k_mg_sweep3v<T, false, true>), gv, 256, st, op, x, f, color,
-                               inh ? 1 : 0, ig, gcv, xc);
+                        { if (two) VD_SWEEP3V(false, true, 2); else VD_SWEEP3V(false, true, 1); }
                     else
-                        LAUNCH((k_mg_sweep3v<T, false, false>), gv, 256, st, op, x, f, color,
-                               inh ? 1 : 0, ig, gcv, xc);
+                        { if (two) VD_SWEEP3V(false, false, 2); else VD_SWEEP3V(false, false, 1); }
+#undef VD_SWEEP3V
                 } else if (op.b[0])
                 {
                     if (pro)
@@ -966,7 +967,7 @@ void explicit_rhs(Ctx& c, double time)
         t_prof->begin(c.st);
     }
     // streaming kernel: one launch per group of EX_QB components
-    const int zc = (cfg.dim == 3) ? std::min(32, c.g.n[2]) : 1;
+    const int zc = (cfg.dim == 3) ? std::min(EX_ZC, c.g.n[2]) : 1;
     const dim3 grid((c.g.n[0] + EX_TX - 1) / EX_TX, (c.g.n[1] + EX_TY - 1) / EX_TY,
                     (c.g.n[2] + zc - 1) / zc);
     for (int q0 = 0; q0 < std::max(n, 1); q0 += EX_QB)

@@ -704,10 +704,11 @@ __device__ __forceinline__ T mg3_gs_value(const MGOp<T>& L, int i, int j, int k,
 // 16-byte (two-element) loads and stores: of a pair's x neighbours three
 // are distinct (one vector and one scalar load), and its y, z neighbours
 // and f are vectors.  Needs nx % 4 == 0 (pairs never straddle a row and
-// rows start 16-byte aligned).  Blocks of 32 pairs by 8 rows, MG3_U planes
-// per thread; warps with a row or plane on the level boundary update their
-// cells one by one with the ghost closure.
-template <typename T, bool VARB, bool PROL>
+// rows start 16-byte aligned).  Blocks of 32 pairs by 8 rows, MG3_UV planes
+// per thread (2 on the finest levels, 1 on smaller ones, where more CTAs
+// matter more: measured); warps with a row or plane on the level boundary
+// update their cells one by one with the ghost closure.
+template <typename T, bool VARB, bool PROL, int MG3_UV>
 __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ MGOp<T> L,
                                                        T* __restrict__ x,
                                                        const T* __restrict__ f, int color,
@@ -722,22 +723,22 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
     const int nx = g.n[0], nxh = nx >> 1, ny = g.n[1], nz = g.n[2];
     const int pr = blockIdx.x * 32 + (threadIdx.x & 31); // pair index: half-cells 2pr, 2pr+1
     const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
-    const int k0 = blockIdx.z * MG3_U;
+    const int k0 = blockIdx.z * MG3_UV;
     const bool active = 2 * pr < nxh && j < ny;
     const long long half = g.ncell() >> 1;
     T* __restrict__ xs = x + color * half;
     const T* __restrict__ xo = x + (1 - color) * half;
     const T* __restrict__ fs = f + color * half;
-    const bool edge = active && (j == 0 || j == ny - 1 || k0 == 0 || k0 + MG3_U > nz - 1);
+    const bool edge = active && (j == 0 || j == ny - 1 || k0 == 0 || k0 + MG3_UV > nz - 1);
     if (!__any_sync(0xffffffffu, edge))
     {
         if (!active) return;
         const int plane = nxh * ny;
         const int hb = 2 * pr + nxh * (j + ny * k0);
-        V2 vx[MG3_U], vym[MG3_U], vyp[MG3_U], vzm[MG3_U], vzp[MG3_U], vf[MG3_U];
-        T sx[MG3_U];
+        V2 vx[MG3_UV], vym[MG3_UV], vyp[MG3_UV], vzm[MG3_UV], vzp[MG3_UV], vf[MG3_UV];
+        T sx[MG3_UV];
 #pragma unroll
-        for (int u = 0; u < MG3_U; ++u)
+        for (int u = 0; u < MG3_UV; ++u)
         {
             const int q = (j + k0 + u + color) & 1;
             const int h = hb + u * plane;
@@ -756,11 +757,11 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
         // prolongation on the fly: an other-colour neighbour at half-index
         // h' of row j has coarse column h'; cells A, B (coarse columns 2pr,
         // 2pr+1) share their y and z neighbours' coarse rows and planes
-        T cxv[MG3_U][3], cyz[MG3_U][8];
+        T cxv[MG3_UV][3], cyz[MG3_UV][8];
         if (PROL)
         {
 #pragma unroll
-            for (int u = 0; u < MG3_U; ++u)
+            for (int u = 0; u < MG3_UV; ++u)
             {
                 const int k = k0 + u;
                 const int q = (j + k + color) & 1;
@@ -785,7 +786,7 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
             }
         }
 #pragma unroll
-        for (int u = 0; u < MG3_U; ++u)
+        for (int u = 0; u < MG3_UV; ++u)
         {
             const int k = k0 + u;
             const int q = (j + k + color) & 1;
@@ -846,7 +847,7 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
     if (!active) return;
     // boundary rows and planes: cell by cell
 #pragma unroll 1
-    for (int u = 0; u < MG3_U; ++u)
+    for (int u = 0; u < MG3_UV; ++u)
     {
         const int k = k0 + u;
         if (k >= nz) break;
