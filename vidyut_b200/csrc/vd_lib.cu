@@ -52,6 +52,29 @@ dim3 gsz(long long n)
         VD_CUDA_OK(cudaGetLastError());                                           \
     } while (0)
 
+// Launch as a programmatic dependent launch: the kernel may be scheduled
+// while the previous kernel on the stream drains, hiding the launch latency
+// that dominates the small multigrid levels.  Only for kernels that begin
+// with VD_PDL_WAIT() (the multigrid kernels of vd_mg.cuh).
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*k)(KArgs...), dim3 g, dim3 b, size_t smem, cudaStream_t st,
+                Args&&... args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = g;
+    cfg.blockDim = b;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    VD_CUDA_OK(cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...));
+    ++vd::g_launches;
+}
+#define LAUNCH_PDL(K, G, B, STREAM, ...) launch_pdl(K, G, B, 0, STREAM, __VA_ARGS__)
+
 // Launch-by-launch event timing of one selected kernel.
 struct Prof
 {
@@ -303,7 +326,7 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                     const dim3 gv((op.g.n[0] / 2 + 63) / 64, grid.y, (op.g.n[2] + uv - 1) / uv);
                     const T ig = op.b[0] ? T(0) : T(1) / gamma;
 #define VD_SWEEP3V(VB, PR, UV)                                                                \
-    LAUNCH((k_mg_sweep3v<T, VB, PR, UV>), gv, 256, st, op, x, f, color, inh ? 1 : 0, ig, gcv, xc)
+    LAUNCH_PDL((k_mg_sweep3v<T, VB, PR, UV>), gv, 256, st, op, x, f, color, inh ? 1 : 0, ig, gcv, xc)
                     if (op.b[0] && pro)
                         { if (two) VD_SWEEP3V(true, true, 2); else VD_SWEEP3V(true, true, 1); }
                     else if (op.b[0])
@@ -316,18 +339,18 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                 } else if (op.b[0])
                 {
                     if (pro)
-                        LAUNCH((k_mg_sweep3<T, true, true>), grid, 256, st, op, x, f, color,
+                        LAUNCH_PDL((k_mg_sweep3<T, true, true>), grid, 256, st, op, x, f, color,
                                inh ? 1 : 0, T(0), gcv, xc);
                     else
-                        LAUNCH((k_mg_sweep3<T, true, false>), grid, 256, st, op, x, f, color,
+                        LAUNCH_PDL((k_mg_sweep3<T, true, false>), grid, 256, st, op, x, f, color,
                                inh ? 1 : 0, T(0), gcv, xc);
                 } else
                 {
                     if (pro)
-                        LAUNCH((k_mg_sweep3<T, false, true>), grid, 256, st, op, x, f, color,
+                        LAUNCH_PDL((k_mg_sweep3<T, false, true>), grid, 256, st, op, x, f, color,
                                inh ? 1 : 0, T(1) / gamma, gcv, xc);
                     else
-                        LAUNCH((k_mg_sweep3<T, false, false>), grid, 256, st, op, x, f, color,
+                        LAUNCH_PDL((k_mg_sweep3<T, false, false>), grid, 256, st, op, x, f, color,
                                inh ? 1 : 0, T(1) / gamma, gcv, xc);
                 }
             } else if (op.g.rb && op.g.dim == 3 && op.g.n[0] >= 4 && op.g.n[1] >= 4 &&
@@ -338,10 +361,10 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                 const int by = 256 / bx;
                 const dim3 grid((nxh + bx - 1) / bx, (op.g.n[1] + by - 1) / by, op.g.n[2]);
                 if (op.b[0])
-                    LAUNCH((k_mg_smooth_rb3<T, true>), grid, dim3(bx, by), st, op, x, f, color,
+                    LAUNCH_PDL((k_mg_smooth_rb3<T, true>), grid, dim3(bx, by), st, op, x, f, color,
                            inh ? 1 : 0, T(0));
                 else
-                    LAUNCH((k_mg_smooth_rb3<T, false>), grid, dim3(bx, by), st, op, x, f,
+                    LAUNCH_PDL((k_mg_smooth_rb3<T, false>), grid, dim3(bx, by), st, op, x, f,
                            color, inh ? 1 : 0, T(1) / gamma);
             } else if (op.g.rb)
             {
@@ -349,13 +372,13 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                 const int bx = nxh >= 128 ? 128 : (nxh >= 64 ? 64 : 32);
                 const dim3 grid((nxh + bx - 1) / bx, op.g.n[1], op.g.n[2]);
                 if (op.b[0])
-                    LAUNCH((k_mg_smooth_rb<T, true>), grid, bx, st, op, x, f, color,
+                    LAUNCH_PDL((k_mg_smooth_rb<T, true>), grid, bx, st, op, x, f, color,
                            inh ? 1 : 0, T(0));
                 else
-                    LAUNCH((k_mg_smooth_rb<T, false>), grid, bx, st, op, x, f, color,
+                    LAUNCH_PDL((k_mg_smooth_rb<T, false>), grid, bx, st, op, x, f, color,
                            inh ? 1 : 0, T(1) / gamma);
             } else
-                LAUNCH(k_mg_smooth_color<T>, gsz(half), BS, st, op, x, f, color, inh ? 1 : 0);
+                LAUNCH_PDL(k_mg_smooth_color<T>, gsz(half), BS, st, op, x, f, color, inh ? 1 : 0);
             if (prof) t_prof->end(st);
         }
 }
@@ -375,7 +398,7 @@ Grid3 rows3(const GridDev& g, int ydiv = 1)
 template <typename T>
 void bottom(Hier<T>& H, const MGOp<T>& op, T* x, const T* f, cudaStream_t st)
 {
-    LAUNCH(k_mg_bottom<T>, 1, 256, st, op, x, f, H.scratch, T(H.bot_rel), H.bot_maxiter,
+    LAUNCH_PDL(k_mg_bottom<T>, 1, 256, st, op, x, f, H.scratch, T(H.bot_rel), H.bot_maxiter,
            H.nub, H.nuf, H.status);
 }
 
@@ -417,15 +440,15 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
             const GridDev& gc = H.g[l + 1];
             const dim3 grid((gc.n[0] + 31) / 32, (gc.n[1] + 7) / 8, gc.n[2]);
             if (H.op[l].b[0])
-                LAUNCH((k_mg_restrict3<T, true>), grid, 256, st, H.op[l], xl, fl, gc,
+                LAUNCH_PDL((k_mg_restrict3<T, true>), grid, 256, st, H.op[l], xl, fl, gc,
                        H.f[l + 1], H.x[l + 1], inh ? 1 : 0);
             else
-                LAUNCH((k_mg_restrict3<T, false>), grid, 256, st, H.op[l], xl, fl, gc,
+                LAUNCH_PDL((k_mg_restrict3<T, false>), grid, 256, st, H.op[l], xl, fl, gc,
                        H.f[l + 1], H.x[l + 1], inh ? 1 : 0);
             continue;
         }
         const Grid3 gr = rows3(H.g[l + 1]);
-        LAUNCH(k_mg_resid_restrict<T>, gr.g, gr.b, st, H.op[l], xl, fl, H.g[l + 1], H.f[l + 1],
+        LAUNCH_PDL(k_mg_resid_restrict<T>, gr.g, gr.b, st, H.op[l], xl, fl, H.g[l + 1], H.f[l + 1],
                H.x[l + 1], inh ? 1 : 0);
     }
     if (lc == L - 1)
@@ -454,20 +477,20 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         if (c3 && smem3 <= VD_MG_COARSE_SMEM)
         {
             if (H.varb)
-                k_mg_coarse3<T, true><<<1, MGC_THREADS, smem3, st>>>(
-                    C, T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf);
+                launch_pdl(k_mg_coarse3<T, true>, dim3(1), dim3(MGC_THREADS), smem3, st, C,
+                           T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf);
             else
-                k_mg_coarse3<T, false><<<1, MGC_THREADS, smem3, st>>>(
-                    C, T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf);
+                launch_pdl(k_mg_coarse3<T, false>, dim3(1), dim3(MGC_THREADS), smem3, st, C,
+                           T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf);
         } else
         {
             const size_t smem = mg_coarse_smem(C);
             const int on_chip = smem <= VD_MG_COARSE_SMEM ? 1 : 0;
             k_mg_coarse_vcycle<T><<<1, 512, on_chip ? smem : 0, st>>>(
                 C, H.scratch, T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf, on_chip);
+            ++vd::g_launches;
+            VD_CUDA_OK(cudaGetLastError());
         }
-        ++vd::g_launches;
-        VD_CUDA_OK(cudaGetLastError());
     }
     for (int l = lc - 1; l >= 0; --l)
     {
@@ -482,7 +505,7 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
                 // rewrites colour 0 without reading it
                 const dim3 grid = mg3_grid(H.g[l]);
                 const dim3 gv((H.g[l].n[0] / 2 + 63) / 64, grid.y, grid.z);
-                LAUNCH(k_mg_prolong_c1<T>, gv, 256, st, H.g[l], H.g[l + 1], xl,
+                LAUNCH_PDL(k_mg_prolong_c1<T>, gv, 256, st, H.g[l], H.g[l + 1], xl,
                        (const T*)H.x[l + 1], H.op[l].stop);
                 smooth(H.op[l], xl, fl, inh, H.nu2, st, l == 0 ? H.prof_tag : VD_PROF_NONE);
             } else
@@ -491,7 +514,7 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
             continue;
         }
         const Grid3 gp = rows3(H.g[l]);
-        LAUNCH(k_mg_prolong_add<T>, gp.g, gp.b, st, H.g[l], H.g[l + 1], xl, H.x[l + 1],
+        LAUNCH_PDL(k_mg_prolong_add<T>, gp.g, gp.b, st, H.g[l], H.g[l + 1], xl, H.x[l + 1],
                H.op[l].stop);
         smooth(H.op[l], xl, fl, inh, H.nu2, st, l == 0 ? H.prof_tag : VD_PROF_NONE);
     }
@@ -630,23 +653,23 @@ void launch_norm(Ctx& c, const MGOp<T>& op, const T* x, const T* f, T* rout, boo
         {
             // pairs of half-cells per thread, 16-byte accesses
             if (op.b[0])
-                LAUNCH((k_mg_resid3v<T, true>), gv, 256, c.st, op, x, f, rout, inh ? 1 : 0,
+                LAUNCH_PDL((k_mg_resid3v<T, true>), gv, 256, c.st, op, x, f, rout, inh ? 1 : 0,
                        both ? 1 : 0, fnorm ? 1 : 0, c.dpart, r32, x32, rscale);
             else
-                LAUNCH((k_mg_resid3v<T, false>), gv, 256, c.st, op, x, f, rout, inh ? 1 : 0,
+                LAUNCH_PDL((k_mg_resid3v<T, false>), gv, 256, c.st, op, x, f, rout, inh ? 1 : 0,
                        both ? 1 : 0, fnorm ? 1 : 0, c.dpart, r32, x32, rscale);
-            LAUNCH(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nbv, fnorm ? 1 : 0, mx);
+            LAUNCH_PDL(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nbv, fnorm ? 1 : 0, mx);
             return;
         }
         if (nb <= c.npart)
         {
             if (op.b[0])
-                LAUNCH((k_mg_resid3<T, true>), grid, 256, c.st, op, x, f, rout, inh ? 1 : 0,
+                LAUNCH_PDL((k_mg_resid3<T, true>), grid, 256, c.st, op, x, f, rout, inh ? 1 : 0,
                        both ? 1 : 0, fnorm ? 1 : 0, c.dpart, r32, x32, rscale);
             else
-                LAUNCH((k_mg_resid3<T, false>), grid, 256, c.st, op, x, f, rout, inh ? 1 : 0,
+                LAUNCH_PDL((k_mg_resid3<T, false>), grid, 256, c.st, op, x, f, rout, inh ? 1 : 0,
                        both ? 1 : 0, fnorm ? 1 : 0, c.dpart, r32, x32, rscale);
-            LAUNCH(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nb, fnorm ? 1 : 0, mx);
+            LAUNCH_PDL(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nb, fnorm ? 1 : 0, mx);
             return;
         }
     }
@@ -654,9 +677,9 @@ void launch_norm(Ctx& c, const MGOp<T>& op, const T* x, const T* f, T* rout, boo
     {
         const long long half = op.g.ncell() >> 1;
         const long long nb = std::min<long long>((half + 255) / 256, c.npart);
-        LAUNCH(k_mg_resid_norm_rb<T>, dim3((unsigned)nb), 256, c.st, op, x, f, rout,
+        LAUNCH_PDL(k_mg_resid_norm_rb<T>, dim3((unsigned)nb), 256, c.st, op, x, f, rout,
                inh ? 1 : 0, fnorm ? 1 : 0, c.dpart);
-        LAUNCH(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nb, fnorm ? 1 : 0, mx);
+        LAUNCH_PDL(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nb, fnorm ? 1 : 0, mx);
         return;
     }
     int rows = 8;
@@ -667,9 +690,9 @@ void launch_norm(Ctx& c, const MGOp<T>& op, const T* x, const T* f, T* rout, boo
         gn = rows3(op.g, rows);
     }
     const long long nb = (long long)gn.g.x * gn.g.y * gn.g.z;
-    LAUNCH(k_mg_resid_norm<T>, gn.g, gn.b, c.st, op, x, f, rout, mx, inh ? 1 : 0,
+    LAUNCH_PDL(k_mg_resid_norm<T>, gn.g, gn.b, c.st, op, x, f, rout, mx, inh ? 1 : 0,
            fnorm ? 1 : 0, rows, c.dpart);
-    LAUNCH(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nb, fnorm ? 1 : 0, mx);
+    LAUNCH_PDL(k_mg_max_partials<T>, 1, 1024, c.st, op, c.dpart, nb, fnorm ? 1 : 0, mx);
 }
 
 template <typename T>
@@ -776,11 +799,11 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
                     launch_norm(c, op0, (const double*)sol, (const double*)rhs, (double*)nullptr,
                                 true, false, &c.dmg->rbits, true, H32.f[0], H32.x[0],
                                 &c.dmg->sc_cur);
-                    LAUNCH(k_ref_check, 1, 1, c.st, c.dmg, target);
+                    LAUNCH_PDL(k_ref_check, 1, 1, c.st, c.dmg, target);
                     for (int q = 0; q < inner; ++q) vcycle(H32, H32.x[0], H32.f[0], false, c.dscal, c.st);
-                    LAUNCH(k_ref_add, gsz(n), BS, c.st, sol, (const float*)H32.x[0],
+                    LAUNCH_PDL(k_ref_add, gsz(n), BS, c.st, sol, (const float*)H32.x[0],
                            (const MGDev*)c.dmg, n);
-                    LAUNCH(k_ref_rotate, 1, 1, c.st, c.dmg, inner);
+                    LAUNCH_PDL(k_ref_rotate, 1, 1, c.st, c.dmg, inner);
                     ++issued;
                 }
                 VD_CUDA_OK(cudaMemcpyAsync(c.hmg, c.dmg, sizeof(MGDev), cudaMemcpyDeviceToHost, c.st));
@@ -793,7 +816,7 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
                 // the last pass's update has no residual check yet: take it
                 launch_norm(c, op0, (const double*)sol, (const double*)rhs, (double*)nullptr,
                             true, false, &c.dmg->rbits, true, H32.f[0], H32.x[0], &c.dmg->sc_cur);
-                LAUNCH(k_ref_check, 1, 1, c.st, c.dmg, target);
+                LAUNCH_PDL(k_ref_check, 1, 1, c.st, c.dmg, target);
                 VD_CUDA_OK(cudaMemcpyAsync(c.hmg, c.dmg, sizeof(MGDev), cudaMemcpyDeviceToHost, c.st));
                 VD_CUDA_OK(cudaStreamSynchronize(c.st));
             }
@@ -812,8 +835,8 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
             while (st.iterations < cfg.linsolve_maxiter)
             {
                 const double s = 1.0 / rn;
-                LAUNCH((k_convert<float, double>), gsz(n), BS, c.st, H32.f[0], c.r64, s, n);
-                LAUNCH(k_fill<float>, gsz(n), BS, c.st, H32.x[0], 0.0f, n);
+                LAUNCH_PDL((k_convert<float, double>), gsz(n), BS, c.st, H32.f[0], c.r64, s, n);
+                LAUNCH_PDL(k_fill<float>, gsz(n), BS, c.st, H32.x[0], 0.0f, n);
                 for (int q = 0; q < inner; ++q)
                 {
                     vcycle(H32, H32.x[0], H32.f[0], false, c.dscal, c.st);
@@ -849,7 +872,7 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
                     // cells then have no residual: only colour 0 is scanned
                     launch_norm(c, op0, (const double*)sol, (const double*)rhs, (double*)nullptr,
                                 true, false, &c.dmg->rbits, H64.nu2 < 1);
-                    LAUNCH(k_mg_check, 1, 1, c.st, c.dmg, target);
+                    LAUNCH_PDL(k_mg_check, 1, 1, c.st, c.dmg, target);
                     ++issued;
                 }
                 VD_CUDA_OK(cudaMemcpyAsync(c.hmg, c.dmg, sizeof(MGDev), cudaMemcpyDeviceToHost, c.st));

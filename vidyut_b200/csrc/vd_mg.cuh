@@ -21,6 +21,12 @@
 #include "vd_common.cuh"
 #include <vector>
 
+// Every multigrid kernel begins by waiting for the grids it depends on:
+// launched with programmatic stream serialization (a dependent launch that
+// may start while the previous kernel drains) it must not read before
+// that kernel's writes are visible; launched normally the wait is a no-op.
+#define VD_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
+
 namespace vd {
 
 enum MGBCType
@@ -204,6 +210,7 @@ template <typename T>
 __global__ void k_mg_smooth_color(MGOp<T> L, T* __restrict__ x,
                                   const T* __restrict__ f, int color, int inhomog)
 {
+    VD_PDL_WAIT();
     if (mg_stopped(L)) return;
     const int nxh = (L.g.n[0] + 1) >> 1;
     const long long tot = (long long)nxh * L.g.n[1] * L.g.n[2];
@@ -230,6 +237,7 @@ __global__ void __launch_bounds__(128) k_mg_smooth_rb(MGOp<T> L, T* __restrict__
                                                       const T* __restrict__ f, int color,
                                                       int inhomog, T inv_gamma)
 {
+    VD_PDL_WAIT();
     if (mg_stopped(L)) return;
     const GridDev& g = L.g;
     const int nxh = g.n[0] >> 1;
@@ -299,6 +307,7 @@ __global__ void __launch_bounds__(256) k_mg_smooth_rb3(MGOp<T> L, T* __restrict_
                                                        const T* __restrict__ f, int color,
                                                        int inhomog, T inv_gamma)
 {
+    VD_PDL_WAIT();
     if (mg_stopped(L)) return;
     const GridDev& g = L.g;
     const int nx = g.n[0], nxh = nx >> 1, ny = g.n[1], nz = g.n[2];
@@ -487,6 +496,7 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3(const __grid_constant__ MG
                                                       int inhomog, T inv_gamma, GridDev gc,
                                                       const T* __restrict__ xc)
 {
+    VD_PDL_WAIT();
     // the stop flag only changes between kernels: a read-only (cached) load
     const int stop = L.stop ? __ldg(L.stop) : 0;
     if (stop) return;
@@ -715,6 +725,7 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
                                                        int inhomog, T inv_gamma, GridDev gc,
                                                        const T* __restrict__ xc)
 {
+    VD_PDL_WAIT();
     using V2 = typename Vec2<T>::type;
     // the stop flag only changes between kernels: a read-only (cached) load
     const int stop = L.stop ? __ldg(L.stop) : 0;
@@ -890,6 +901,7 @@ __global__ void __launch_bounds__(256) k_mg_prolong_c1(GridDev g, GridDev gc, T*
                                                        const T* __restrict__ xc,
                                                        const int* stop)
 {
+    VD_PDL_WAIT();
     using V2 = typename Vec2<T>::type;
     if (stop && *(volatile const int*)stop) return;
     const int nxh = g.n[0] >> 1, ny = g.n[1], nz = g.n[2];
@@ -950,6 +962,7 @@ __global__ void __launch_bounds__(256, 3) k_mg_restrict3(const __grid_constant__
                                                       T* __restrict__ fc, T* __restrict__ xc,
                                                       int inhomog)
 {
+    VD_PDL_WAIT();
     // the stop flag only changes between kernels: a read-only (cached) load
     const int stop = L.stop ? __ldg(L.stop) : 0;
     if (stop) return;
@@ -1070,6 +1083,7 @@ __global__ void __launch_bounds__(256, 4) k_mg_resid3v(const __grid_constant__ M
                                                        float* __restrict__ x32 = nullptr,
                                                        const double* rscale = nullptr)
 {
+    VD_PDL_WAIT();
     using V2 = typename Vec2<T>::type;
     __shared__ double sh[32];
     const int stop = L.stop ? __ldg(L.stop) : 0;
@@ -1226,6 +1240,7 @@ __global__ void __launch_bounds__(256, 4) k_mg_resid3(const __grid_constant__ MG
                                                       float* __restrict__ x32 = nullptr,
                                                       const double* rscale = nullptr)
 {
+    VD_PDL_WAIT();
     __shared__ double sh[32];
     // the stop flag only changes between kernels: a read-only (cached) load
     const int stop = L.stop ? __ldg(L.stop) : 0;
@@ -1415,6 +1430,7 @@ __global__ void __launch_bounds__(128) k_mg_resid_restrict(MGOp<T> L, const T* _
                                                            T* __restrict__ fc,
                                                            T* __restrict__ xc, int inhomog)
 {
+    VD_PDL_WAIT();
     if (mg_stopped(L)) return;
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= gc.n[0]) return;
@@ -1447,6 +1463,7 @@ __global__ void __launch_bounds__(128) k_mg_resid_norm(MGOp<T> L, const T* __res
                                                        int fnorm, int rows,
                                                        double* part = nullptr)
 {
+    VD_PDL_WAIT();
     if (mg_stopped(L)) return;
     __shared__ double sh[32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1498,6 +1515,7 @@ __global__ void __launch_bounds__(256) k_mg_resid_norm_rb(MGOp<T> L, const T* __
                                                           T* __restrict__ rout, int inhomog,
                                                           int fnorm, double* __restrict__ part)
 {
+    VD_PDL_WAIT();
     if (mg_stopped(L)) return;
     __shared__ double sh[32];
     const GridDev& g = L.g;
@@ -1542,6 +1560,7 @@ __global__ void __launch_bounds__(1024) k_mg_max_partials(MGOp<T> L, const doubl
                                                           long long nb, int fnorm,
                                                           unsigned long long* mx)
 {
+    VD_PDL_WAIT();
     if (mg_stopped(L)) return;
     __shared__ double sh[32];
     double m = 0.0, mf = 0.0;
@@ -1565,6 +1584,7 @@ __global__ void __launch_bounds__(128) k_mg_prolong_add(GridDev gf, GridDev gc,
                                                         const T* __restrict__ xc,
                                                         const int* stop)
 {
+    VD_PDL_WAIT();
     if (stop && *(volatile const int*)stop) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= gf.n[0]) return;
@@ -1715,6 +1735,7 @@ __global__ void k_mg_bottom(MGOp<T> L, T* __restrict__ x, const T* __restrict__ 
                             T* __restrict__ scr, T rel, int maxiter, int nub, int nuf,
                             int* status)
 {
+    VD_PDL_WAIT();
     if (mg_stopped(L)) return;
     __shared__ T sh[32];
     mg_bottom_block(L, x, b, scr, rel, maxiter, nub, nuf, status, sh);
@@ -1777,6 +1798,7 @@ __global__ void __launch_bounds__(512) k_mg_coarse_vcycle(MGCoarse<T> C, T* __re
                                                           T rel, int maxiter, int nu1, int nu2,
                                                           int nub, int nuf, int on_chip)
 {
+    VD_PDL_WAIT();
     extern __shared__ __align__(16) unsigned char mg_smem[];
     if (mg_stopped(C.op[C.lc])) return;
     __shared__ T sh[32];
@@ -1955,6 +1977,7 @@ template <typename T, bool VARB>
 __global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3(MGCoarse<T> C, T rel, int maxiter,
                                                             int nu1, int nu2, int nub, int nuf)
 {
+    VD_PDL_WAIT();
     extern __shared__ __align__(16) unsigned char mgc_smem[];
     __shared__ T sh[32];
     if (mg_stopped(C.op[C.lc])) return;
@@ -2080,6 +2103,7 @@ template <typename T>
 __global__ void k_mg_avg_faces(GridDev gf, GridDev gc, int d, const T* __restrict__ bf,
                                T* __restrict__ bc)
 {
+    VD_PDL_WAIT();
     const long long tot = face_count(gc, d);
     const int rz = (gf.dim == 3) ? 2 : 1;
     const int nx = gc.n[0] + (d == 0), ny = gc.n[1] + (d == 1);
@@ -2112,6 +2136,7 @@ template <typename T>
 __global__ void k_mg_robin_coarsen(GridDev gf, GridDev gc, int s, const T* ra_f,
                                    const T* rb_f, T* ra_c, T* rb_c, T* c0_c, T dxc)
 {
+    VD_PDL_WAIT();
     const int d = s % 3;
     const int ta = (d == 0) ? 1 : 0, tb = (d == 2) ? 1 : 2;
     const int na = gc.n[ta], nb = gc.n[tb];
@@ -2143,6 +2168,7 @@ __global__ void k_mg_robin_coarsen(GridDev gf, GridDev gc, int s, const T* ra_f,
 template <typename T>
 __global__ void k_fill(T* p, T v, long long n)
 {
+    VD_PDL_WAIT();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x)
         p[t] = v;
@@ -2151,6 +2177,7 @@ __global__ void k_fill(T* p, T v, long long n)
 template <typename TO, typename TI>
 __global__ void k_convert(TO* __restrict__ o, const TI* __restrict__ in, TI scale, long long n)
 {
+    VD_PDL_WAIT();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x)
         o[t] = (TO)(in[t] * scale);
@@ -2176,6 +2203,7 @@ struct MGDev
 // meets the target (nothing happens once the flag is up).
 __global__ void k_mg_check(MGDev* s, double target)
 {
+    VD_PDL_WAIT();
     if (s->done) return;
     s->iters += 1;
     s->final_bits = s->rbits;
@@ -2187,6 +2215,7 @@ __global__ void k_mg_check(MGDev* s, double target)
 // next right-hand side scale.
 __global__ void k_ref_check(MGDev* s, double target)
 {
+    VD_PDL_WAIT();
     if (s->done) return;
     s->final_bits = s->rbits;
     const double r = __longlong_as_double((long long)s->rbits);
@@ -2200,6 +2229,7 @@ __global__ void k_ref_check(MGDev* s, double target)
 __global__ void k_ref_add(double* __restrict__ x, const float* __restrict__ e, const MGDev* s,
                           long long n)
 {
+    VD_PDL_WAIT();
     if (*(volatile const int*)&s->done) return;
     const double inv = 1.0 / s->sc_cur;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
@@ -2210,6 +2240,7 @@ __global__ void k_ref_add(double* __restrict__ x, const float* __restrict__ e, c
 // One refinement pass completed: count it and move to the next scale.
 __global__ void k_ref_rotate(MGDev* s, int inner)
 {
+    VD_PDL_WAIT();
     if (s->done) return;
     s->refs += 1;
     s->iters += inner;
