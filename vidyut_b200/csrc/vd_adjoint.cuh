@@ -143,6 +143,7 @@ __device__ __forceinline__ bool adj_wall(const AdjParams& P, int s, int d, bool 
 // Mobilities and their density derivatives of every transported species.
 __global__ void __launch_bounds__(256) k_adj_props(AdjParams P, const double* __restrict__ u)
 {
+    VD_PDL_WAIT();
     const long long N = P.g.ncell();
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < N;
          q += (long long)gridDim.x * blockDim.x)
@@ -174,6 +175,7 @@ __global__ void __launch_bounds__(256) k_adj_props(AdjParams P, const double* __
 __global__ void __launch_bounds__(256) k_adj_step(AdjParams P, const double* __restrict__ u,
                                                   double* __restrict__ unew)
 {
+    VD_PDL_WAIT();
     const GridDev& g = P.g;
     const long long N = g.ncell();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
@@ -223,6 +225,7 @@ __global__ void __launch_bounds__(128) k_adj_faces(AdjParams P, int d,
                                                    double* __restrict__ adj,
                                                    double* __restrict__ adjnd, double* gmob)
 {
+    VD_PDL_WAIT();
     __shared__ double sh[32];
     const GridDev& g = P.g;
     const long long N = g.ncell();
@@ -311,6 +314,7 @@ __global__ void __launch_bounds__(128) k_adj_chem_update(AdjParams P,
                                                          const double* __restrict__ adjnd,
                                                          double* gtheta)
 {
+    VD_PDL_WAIT();
     __shared__ double sh[32];
     const long long N = P.g.ncell();
     double gl[NUM_REACTIONS];
@@ -410,6 +414,7 @@ __device__ __forceinline__ void dd_block_sum(double& hi, double& lo, double* sh)
 __global__ void k_adj_objective(long long n, const double* __restrict__ ue,
                                 double* __restrict__ part)
 {
+    VD_PDL_WAIT();
     __shared__ double sh[64];
     double hi = 0.0, lo = 0.0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
@@ -427,6 +432,7 @@ __global__ void k_adj_objective(long long n, const double* __restrict__ ue,
 __global__ void k_adj_objective_final(int nb, const double* __restrict__ part, double dv,
                                       double* J)
 {
+    VD_PDL_WAIT();
     __shared__ double sh[64];
     double hi = 0.0, lo = 0.0;
     for (int b = threadIdx.x; b < nb; b += blockDim.x) dd_add_dd(hi, lo, part[2 * b], part[2 * b + 1]);

@@ -14,6 +14,13 @@
             throw vd::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
+// Every kernel of the library begins by waiting for the grids it depends
+// on: launched with programmatic stream serialization (a dependent launch
+// that may be scheduled while the previous kernel drains) it must not read
+// before that kernel's writes are visible; launched normally the wait is a
+// no-op.
+#define VD_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
+
 namespace vd {
 
 struct CudaError

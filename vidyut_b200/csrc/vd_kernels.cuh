@@ -98,6 +98,7 @@ __global__ void k_poisson_rhs(Geo G, GridDev gm, const double* __restrict__ Sold
                               int do_spacechrg, int warm, double ps, double time,
                               const ProbParm* pp)
 {
+    VD_PDL_WAIT();
     const long long N = G.g.ncell();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
          t += (long long)gridDim.x * blockDim.x)
@@ -143,6 +144,7 @@ __global__ void k_bc_hook(Geo G, int s, int kind, int comp, double* S, SideArray
                           double time, double app_voltage, int user_defined, double Tg,
                           double Pg, const ProbParm* pp)
 {
+    VD_PDL_WAIT();
     const int d = s % 3;
     const int ta = (d == 0) ? 1 : 0, tb = (d == 2) ? 1 : 2;
     const int np = G.g.n[ta] * G.g.n[tb];
@@ -198,6 +200,7 @@ __global__ void k_bc_hook(Geo G, int s, int kind, int comp, double* S, SideArray
 __global__ void k_bc_finalize(int np, int type, int nx_d, int maxorder, double dx,
                               double scale, SideArrays A)
 {
+    VD_PDL_WAIT();
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x)
     {
         A.val[q] *= scale;
@@ -224,6 +227,7 @@ __global__ void k_inneu_adjust(GridDev g, int s, const double* bface, double bco
                                double beta, double dx, const double* val,
                                double* __restrict__ rhs)
 {
+    VD_PDL_WAIT();
     const int d = s % 3;
     const int ta = (d == 0) ? 1 : 0, tb = (d == 2) ? 1 : 2;
     const int np = g.n[ta] * g.n[tb];
@@ -292,6 +296,7 @@ __device__ __forceinline__ double grad_at_face(const GradCtx& C, const double* _
 __global__ void __launch_bounds__(128) k_efield(GradCtx C, const double* __restrict__ sol,
                                                 double* __restrict__ S, double ps)
 {
+    VD_PDL_WAIT();
     const GridDev& g = C.op.g;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.n[0]) return;
@@ -399,6 +404,7 @@ __device__ __forceinline__ void ex_cell_vel(const ExplParams& P, int ci, int cj,
 #endif
 __global__ void __launch_bounds__(256, EX_MINB) k_explicit_stream(ExplParams P, int q0, int zc)
 {
+    VD_PDL_WAIT();
     __shared__ double s_n[EX_QB][EX_HY][EX_HX];
     __shared__ double s_vx[EX_QB][EX_HY][EX_HX];
     __shared__ double s_vy[EX_QB][EX_HY][EX_HX];
@@ -655,6 +661,7 @@ __device__ __forceinline__ double cell_diff(const double* __restrict__ S, const 
 __global__ void k_species_faces(GridDev g, int d, const double* __restrict__ S, int spec,
                                 double Tg, double* __restrict__ bf)
 {
+    VD_PDL_WAIT();
     const long long tot = face_count(g, d);
     const long long N = g.ncell();
     const int nx = g.n[0] + (d == 0), ny = g.n[1] + (d == 1);
@@ -679,6 +686,7 @@ __global__ void k_species_rhs(GridDev g, GridDev gm, const double* __restrict__ 
                               int spec, double dt, double ts, double scale,
                               double* __restrict__ rhs, double* __restrict__ sol)
 {
+    VD_PDL_WAIT();
     const long long N = g.ncell();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
          t += (long long)gridDim.x * blockDim.x)
@@ -738,6 +746,7 @@ __device__ __forceinline__ double onesided_grad(const double* S, const GridDev& 
 
 __global__ void k_joule(JouleParams P)
 {
+    VD_PDL_WAIT();
     // the state is in natural layout; the Poisson level's grid may be red-black
     GridDev g = P.pot.op.g;
     g.rb = 0;
@@ -829,6 +838,7 @@ struct FinalParams
 
 __global__ void k_finalize(FinalParams P)
 {
+    VD_PDL_WAIT();
     const long long N = P.g.ncell();
     double* __restrict__ S = P.S;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
@@ -892,6 +902,7 @@ __global__ void k_finalize(FinalParams P)
 
 __global__ void k_midpoint(double* __restrict__ S, const double* __restrict__ Sold, long long n)
 {
+    VD_PDL_WAIT();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x)
         S[t] = 0.5 * Sold[t] + 0.5 * S[t];
@@ -899,6 +910,7 @@ __global__ void k_midpoint(double* __restrict__ S, const double* __restrict__ So
 
 __global__ void k_nonfinite(const double* __restrict__ S, long long n, unsigned long long* cnt)
 {
+    VD_PDL_WAIT();
     unsigned long long c = 0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x)
@@ -910,6 +922,7 @@ template <typename T>
 __global__ void k_add_same(T* __restrict__ x, const T* __restrict__ e, long long n,
                            const int* stop)
 {
+    VD_PDL_WAIT();
     if (stop && *(volatile const int*)stop) return;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x)
@@ -919,6 +932,7 @@ __global__ void k_add_same(T* __restrict__ x, const T* __restrict__ e, long long
 template <typename T>
 __global__ void k_add_scaled(double* __restrict__ x, const T* __restrict__ e, double s, long long n)
 {
+    VD_PDL_WAIT();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x)
         x[t] += (double)e[t] * s;

@@ -44,13 +44,9 @@ dim3 gsz(long long n)
     return dim3((unsigned)b);
 }
 
-#define LAUNCH(K, G, B, STREAM, ...)                                              \
-    do                                                                            \
-    {                                                                             \
-        K<<<(G), (B), 0, (STREAM)>>>(__VA_ARGS__);                                \
-        ++vd::g_launches;                                                         \
-        VD_CUDA_OK(cudaGetLastError());                                           \
-    } while (0)
+// Every launch is a programmatic dependent launch (launch_pdl below): all
+// kernels of the library start with VD_PDL_WAIT().
+#define LAUNCH(K, G, B, STREAM, ...) launch_pdl(K, G, B, 0, STREAM, __VA_ARGS__)
 
 // Launch as a programmatic dependent launch: the kernel may be scheduled
 // while the previous kernel on the stream drains, hiding the launch latency
@@ -420,7 +416,7 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
     {
         const Grid3 gn = rows3(H.g[0], 8);
         LAUNCH(k_mg_resid_norm<T>, gn.g, gn.b, st, H.op[0], x0, f0, H.t0f, dscr, inh0 ? 1 : 0,
-               0, 8);
+               0, 8, (double*)nullptr);
         bottom(H, H.op[0], H.t0x, H.t0f, st);
         LAUNCH(k_add_same<T>, gsz(H.g[0].ncell()), BS, st, x0, H.t0x, H.g[0].ncell(),
                H.op[0].stop);
@@ -1132,6 +1128,7 @@ void step_once(Ctx& c)
 
 __global__ void k_initdomain(Geo G, double* S, const ProbParm* pp)
 {
+    VD_PDL_WAIT();
     const long long N = G.g.ncell();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
          t += (long long)gridDim.x * blockDim.x)
@@ -2095,6 +2092,7 @@ int na_vcycle(NAHier& H, double* x0, const double* f0, char* err, int errlen)
 
 __global__ void k_na_fill_side(double* g, int np, double v)
 {
+    VD_PDL_WAIT();
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x)
         g[q] = v;
 }

@@ -21,11 +21,6 @@
 #include "vd_common.cuh"
 #include <vector>
 
-// Every multigrid kernel begins by waiting for the grids it depends on:
-// launched with programmatic stream serialization (a dependent launch that
-// may start while the previous kernel drains) it must not read before
-// that kernel's writes are visible; launched normally the wait is a no-op.
-#define VD_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
 
 namespace vd {
 
