@@ -115,3 +115,54 @@ def test_fp32_refined_poisson_error(require_gpu):
     assert sg.converged and so.converged
     pid = g.info["pot_id"]
     assert rel(g.get_state(pid, 1), o.get_state(pid, 1)) < 1e-9
+
+
+# Grids the oracle solves in seconds, with the level-size threshold of the
+# sweeps built for HBM-resident levels lowered to one cell: every red-black
+# level with nx % 4 == 0 then runs the two-planes-per-thread sweeps that
+# otherwise only levels of 8 M cells or more use, FP64 and FP32, constant and
+# face coefficients, with and without the fused prolongation.
+BIG_SHAPES = [(64, 64, 48), (96, 64, 32), (64, 96, 70), (64, 64, 64)]
+
+
+@pytest.mark.parametrize("shape", BIG_SHAPES)
+@pytest.mark.parametrize("bc", BCS[:2])
+def test_poisson_hbm_level_sweeps(require_gpu, monkeypatch, shape, bc):
+    monkeypatch.setenv("VD_MG_BIG_LEVEL_CELLS", "1")
+    g, o = pair(box(*shape, pot_lo=bc[0], pot_hi=bc[1]), 21)
+    sg = g.solve_potential(0.0)
+    so = o.solve_potential(0.0)
+    assert sg.converged and so.converged
+    assert abs(sg.iterations - so.iterations) <= 1, (sg.iterations, so.iterations)
+    pid = g.info["pot_id"]
+    assert rel(g.get_state(pid, 1), o.get_state(pid, 1)) < 1e-11
+
+
+@pytest.mark.parametrize("spec", [0, 1])
+def test_species_solve_hbm_level_sweeps(require_gpu, monkeypatch, spec):
+    monkeypatch.setenv("VD_MG_BIG_LEVEL_CELLS", "1")
+    cfg = box(64, 64, 64)
+    g, o = pair(cfg, 22)
+    o.solve_potential(0.0)
+    g.set_state(0, o.get_state())
+    ex = o.explicit_rhs(0.0)
+    sg = g.implicit_solve_scalar(spec, ex, 0.0)
+    so = o.implicit_solve_scalar(spec, ex, 0.0)
+    assert sg.converged and so.converged
+    assert rel(g.get_state(spec, 1), o.get_state(spec, 1)) < 1e-12
+
+
+def test_fp32_refined_hbm_level_sweeps(require_gpu, monkeypatch):
+    monkeypatch.setenv("VD_MG_BIG_LEVEL_CELLS", "1")
+    cfg = box(64, 64, 64, mg_precision=vb.VD_MG_FP32_REFINED)
+    cfg["linsolve_reltol"] = 1e-10
+    g = vb.Vidyut(cfg)
+    o = Oracle(box(64, 64, 64))
+    state = W.initial_state(cfg, 23)
+    g.set_state(0, state)
+    o.set_state(0, state)
+    sg = g.solve_potential(0.0)
+    so = o.solve_potential(0.0)
+    assert sg.converged and so.converged
+    pid = g.info["pot_id"]
+    assert rel(g.get_state(pid, 1), o.get_state(pid, 1)) < 1e-9

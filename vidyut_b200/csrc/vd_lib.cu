@@ -218,15 +218,28 @@ void hier_build(Hier<T>& H, Alloc& A, const GridDev& fine, const double* dx, int
     H.status = A.get<int>(1);
 }
 
+// Level size from which the multigrid sweeps switch to the kernels built for
+// levels that live in HBM rather than L2 (two planes per thread).
+// The environment variable VD_MG_BIG_LEVEL_CELLS overrides the 8 M default,
+// so that tests can drive those kernels on grids the oracle solves quickly.
+static long long big_level_cells()
+{
+    const char* e = std::getenv("VD_MG_BIG_LEVEL_CELLS");
+    const long long v = e ? std::atoll(e) : 0;
+    return v > 0 ? v : (8LL << 20);
+}
+
 template <typename T>
 void hier_set_ops(Hier<T>& H, double aconst, double beta, double bconst, const int* bct,
                   int maxorder)
 {
     H.op.assign(H.nlev, MGOp<T>{});
+    const long long big = big_level_cells();
     for (int l = 0; l < H.nlev; ++l)
     {
         MGOp<T>& o = H.op[l];
         o.g = H.g[l];
+        o.big_cells = big;
         for (int d = 0; d < 3; ++d)
             o.dh[d] = (d < H.dim) ? T(beta / (H.dx[l][d] * H.dx[l][d])) : T(0);
         o.aconst = T(aconst);
@@ -317,7 +330,8 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                 if (op.g.n[0] % 4 == 0)
                 {
                     // pairs of half-cells per thread, 16-byte accesses
-                    const bool two = op.g.ncell() >= (8LL << 20); // planes per thread
+                    const bool two = op.g.ncell() >= (op.big_cells > 0 ? op.big_cells
+                                                                       : (8LL << 20));
                     const int uv = two ? 2 : 1;
                     const dim3 gv((op.g.n[0] / 2 + 63) / 64, grid.y, (op.g.n[2] + uv - 1) / uv);
                     const T ig = op.b[0] ? T(0) : T(1) / gamma;

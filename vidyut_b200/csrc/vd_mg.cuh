@@ -48,6 +48,8 @@ struct MGOp
     const T* c0[6];
     const T* gv[6];
     const int* stop; // set to non-zero on the device once the solve has converged
+    long long big_cells; // host only: levels of at least this many cells (0: 8 M) take the
+                         // sweeps built for HBM-resident levels
 };
 
 template <typename T>
