@@ -1895,7 +1895,7 @@ struct MGCLevel
     T* f;
     T* G;
     T* iG;
-    int* crd; // i | j << 10 | k << 20
+    int* crd; // i | j << 10 | k << 20; colour-0 cells first when nx is even
 };
 
 // Per-side weights of cell (i,j,k): w[s2] for the neighbour on side s2
@@ -1939,34 +1939,189 @@ __device__ __forceinline__ void mgc_weights(const MGOp<T>& L, int i, int j, int 
         }
 }
 
+// sum_n w_n x_n of cell c with the weights of mgc_weights, formed with
+// selects instead of branches (every warp of a coarse level holds row-end
+// cells, so a branch per side would diverge in all of them): an outside
+// side's weight is 0 and its index the opposite neighbour's, and the
+// opposite weight gains w c1.  Same terms in the same order as mgc_weights
+// gives them.
 template <typename T, bool VARB>
 __device__ __forceinline__ T mgc_sum(const MGOp<T>& L, const T* __restrict__ x, int c, int i,
                                      int j, int k)
 {
-    T w[6], G;
-    int o[6];
-    mgc_weights<T, VARB>(L, i, j, k, w, o, G);
+    const int nx = L.g.n[0], ny = L.g.n[1], nz = L.g.n[2];
+    T b[6];
+    mg3_faces<T, VARB>(L, i, j, k, b);
+    const int st[3] = {1, nx, nx * ny};
+    const int cd[3] = {i, j, k}, n[3] = {nx, ny, nz};
     T s = T(0);
 #pragma unroll
-    for (int m = 0; m < 6; ++m) s += w[m] * x[c + o[m]];
+    for (int d = 0; d < 3; ++d)
+    {
+        const T dh = L.dh[d];
+        const bool lo = cd[d] == 0, hi = cd[d] == n[d] - 1;
+        const T wl = dh * b[2 * d], wh = dh * b[2 * d + 1];
+        const T wl2 = lo ? T(0) : (hi ? wl + wh * L.c1s[d + 3] : wl);
+        const T wh2 = hi ? T(0) : (lo ? wh + wl * L.c1s[d] : wh);
+        const int ol = lo ? st[d] : -st[d], oh = hi ? -st[d] : st[d];
+        s += wl2 * x[c + ol];
+        s += wh2 * x[c + oh];
+    }
     return s;
 }
 
+// nsm Gauss-Seidel iterations on a level held on chip.  With nx even the
+// coordinate list holds each colour's cells contiguously, so a colour sweep
+// visits only its own cells (no lane idles on the other colour).
 template <typename T, bool VARB>
-__device__ void mgc_smooth(const MGOp<T>& L, const MGCLevel<T>& V, int nsm)
+__device__ void mgc_smooth(const MGOp<T>& L, const MGCLevel<T> V, int nsm)
 {
+    const int nx = L.g.n[0], ny = L.g.n[1];
     const int n = (int)L.g.ncell();
+    const bool sorted = (nx & 1) == 0;
+    const int cnt = sorted ? n >> 1 : n;
     for (int sm = 0; sm < nsm; ++sm)
         for (int color = 0; color < 2; ++color)
         {
-            for (int c = threadIdx.x; c < n; c += MGC_THREADS)
+            const int* crd = V.crd + (sorted ? color * cnt : 0);
+            for (int m = threadIdx.x; m < cnt; m += MGC_THREADS)
             {
-                const int cr = V.crd[c];
-                const int i = cr & 1023, j = (cr >> 10) & 1023, k = cr >> 20;
-                if (((i + j + k) & 1) != color) continue;
-                V.x[c] = (V.f[c] + mgc_sum<T, VARB>(L, V.x, c, i, j, k)) * V.iG[c];
+                const int cr = crd[m];
+                const int i = cr & 1023, j = (cr >> 10) & 1023, k = (cr >> 20) & 1023;
+                if (!sorted && ((i + j + k) & 1) != color) continue;
+                const int c = i + nx * (j + ny * k);
+                V.x[c] = (V.f[c] + mgc_sum<T, VARB>(L, V.x, c, i, j, k)) *
+                         V.iG[c];
             }
             __syncthreads();
+        }
+}
+
+// mg_bottom_block (BiCGStab, then nub or nuf Gauss-Seidel iterations) for
+// a bottom level of at most 32 cells, on warp 0 alone: one cell per lane,
+// reductions by warp shuffles, no block barriers (the other warps wait at
+// the caller's barrier).  The operator is the G x0 - sum w x form; p and s
+// go through shared memory (scr) because the operator reads neighbours.
+template <typename T, bool VARB>
+__device__ void mgc_bottom_warp(const MGOp<T>& L, const MGCLevel<T> V, T* __restrict__ scr,
+                                T rel, int maxiter, int nub, int nuf)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int n = (int)L.g.ncell();
+    const int lane = threadIdx.x & 31;
+    const bool act = lane < n;
+    const int nx = L.g.n[0], ny = L.g.n[1];
+    const int c = act ? lane : 0;
+    const int i = c % nx, rr = c / nx, j = rr % ny, k = rr / ny;
+    T w[6], G;
+    int o[6];
+    mgc_weights<T, VARB>(L, i, j, k, w, o, G);
+    T* p = scr;
+    T* sv = scr + n;
+    auto wsum = [&](T v) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(FULL, v, off);
+        return v;
+    };
+    auto wmax = [&](T v) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            const T u = __shfl_xor_sync(FULL, v, off);
+            v = u > v ? u : v;
+        }
+        return v;
+    };
+    auto apply = [&](const T* u) {
+        T s = T(0);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) s += w[m] * u[c + o[m]];
+        return G * u[c] - s;
+    };
+    auto absv = [](T a) { return a < T(0) ? -a : a; };
+    T xv = T(0), rv = act ? V.f[c] : T(0);
+    const T rh = rv;
+    T pv = T(0), vv = T(0);
+    const T rnorm0 = wmax(absv(rv));
+    int ret = 0;
+    if (rnorm0 > T(0))
+    {
+        ret = 8;
+        T rho_1 = T(1), alpha = T(1), omega = T(1);
+        for (int iter = 1; iter <= maxiter; ++iter)
+        {
+            const T rho = wsum(rh * rv);
+            if (rho == T(0))
+            {
+                ret = 1;
+                break;
+            }
+            if (iter == 1)
+                pv = rv;
+            else
+            {
+                const T beta = (rho / rho_1) * (alpha / omega);
+                pv = rv + beta * (pv - omega * vv);
+            }
+            if (act) p[c] = pv;
+            __syncwarp();
+            vv = act ? apply(p) : T(0);
+            __syncwarp();
+            const T rhTv = wsum(rh * vv);
+            if (rhTv == T(0))
+            {
+                ret = 2;
+                break;
+            }
+            alpha = rho / rhTv;
+            xv += alpha * pv;
+            const T sval = rv - alpha * vv;
+            if (wmax(absv(sval)) <= rel * rnorm0)
+            {
+                ret = 0;
+                break;
+            }
+            if (act) sv[c] = sval;
+            __syncwarp();
+            const T tv = act ? apply(sv) : T(0);
+            __syncwarp();
+            const T ttt = wsum(tv * tv);
+            const T tts = wsum(tv * sval);
+            if (ttt == T(0))
+            {
+                ret = 3;
+                break;
+            }
+            omega = tts / ttt;
+            xv += omega * sval;
+            rv = sval - omega * tv;
+            if (wmax(absv(rv)) <= rel * rnorm0)
+            {
+                ret = 0;
+                break;
+            }
+            if (omega == T(0))
+            {
+                ret = 4;
+                break;
+            }
+            rho_1 = rho;
+        }
+    }
+    if (act) V.x[c] = xv;
+    __syncwarp();
+    const int nsm = (ret == 0) ? nub : nuf;
+    for (int sm = 0; sm < nsm; ++sm)
+        for (int color = 0; color < 2; ++color)
+        {
+            if (act && ((i + j + k + color) & 1) == 0)
+            {
+                T s = T(0);
+#pragma unroll
+                for (int m = 0; m < 6; ++m) s += w[m] * V.x[c + o[m]];
+                V.x[c] = (V.f[c] + s) * V.iG[c];
+            }
+            __syncwarp();
         }
 }
 
@@ -2007,7 +2162,11 @@ __global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3(MGCoarse<T> C, T rel
         for (int c = threadIdx.x; c < n; c += MGC_THREADS)
         {
             const int i = c % nx, r = c / nx, j = r % ny, k = r / ny;
-            V[l].crd[c] = i | (j << 10) | (k << 20);
+            // with nx even every row holds nx/2 cells of each colour
+            const int m = (nx & 1) ? c
+                                   : ((i + j + k) & 1) * (n >> 1) + (j + ny * k) * (nx >> 1) +
+                                         (i >> 1);
+            V[l].crd[m] = i | (j << 10) | (k << 20);
             T w[6], G;
             int o[6];
             mgc_weights<T, VARB>(L, i, j, k, w, o, G);
@@ -2026,24 +2185,38 @@ __global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3(MGCoarse<T> C, T rel
     {
         const MGOp<T>& L = C.op[l];
         mgc_smooth<T, VARB>(L, V[l], nu1);
+        const MGCLevel<T> Vf = V[l], Vc = V[l + 1]; // in registers, not the local array
         const GridDev& gc = C.op[l + 1].g;
         const int nx = L.g.n[0], ny = L.g.n[1];
         const int ncx = gc.n[0], ncy = gc.n[1], nc = (int)gc.ncell();
-        for (int cc = threadIdx.x; cc < nc; cc += MGC_THREADS)
+        // g threads per coarse cell (the most that keep the level to one pass
+        // of the block), each summing 8/g children; the g partial sums are
+        // g aligned lanes of one warp, added by shuffles
+        int g = 8;
+        while (g > 1 && nc * g > MGC_THREADS) g >>= 1;
+        const int per = 8 / g;
+        for (int base = 0; base < g * nc; base += MGC_THREADS)
         {
+            const int t = base + threadIdx.x;
+            const bool valid = t < g * nc;
+            const int cc = valid ? t / g : 0, sub = t & (g - 1);
             const int I = cc % ncx, R = cc / ncx, J = R % ncy, K = R / ncy;
-            T s = T(0);
-            for (int kk = 0; kk < 2; ++kk)
-                for (int jj = 0; jj < 2; ++jj)
-                    for (int ii = 0; ii < 2; ++ii)
-                    {
-                        const int i = 2 * I + ii, j = 2 * J + jj, k = 2 * K + kk;
-                        const int c = i + nx * (j + ny * k);
-                        const T ax = V[l].G[c] * V[l].x[c] - mgc_sum<T, VARB>(L, V[l].x, c, i, j, k);
-                        s += V[l].f[c] - ax;
-                    }
-            V[l + 1].f[cc] = s * T(0.125);
-            V[l + 1].x[cc] = T(0);
+            T r = T(0);
+            if (valid)
+                for (int q = 0; q < per; ++q)
+                {
+                    const int ch = sub * per + q;
+                    const int i = 2 * I + (ch & 1), j = 2 * J + ((ch >> 1) & 1),
+                              k = 2 * K + (ch >> 2);
+                    const int c = i + nx * (j + ny * k);
+                    r += Vf.f[c] - (Vf.G[c] * Vf.x[c] - mgc_sum<T, VARB>(L, Vf.x, c, i, j, k));
+                }
+            for (int off = 1; off < g; off <<= 1) r += __shfl_xor_sync(0xffffffffu, r, off);
+            if (valid && sub == 0)
+            {
+                Vc.f[cc] = r * T(0.125);
+                Vc.x[cc] = T(0);
+            }
         }
         __syncthreads();
     }
@@ -2051,8 +2224,13 @@ __global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3(MGCoarse<T> C, T rel
     {
         MGOp<T> Lb = C.op[last];
         Lb.g.rb = 0;
-        mg_bottom_block(Lb, V[last].x, V[last].f, bscr, rel, maxiter, nub, nuf, (int*)nullptr,
-                        sh);
+        if (Lb.g.ncell() <= 32)
+        {
+            if (threadIdx.x < 32) mgc_bottom_warp<T, VARB>(Lb, V[last], bscr, rel, maxiter, nub, nuf);
+            __syncthreads();
+        } else
+            mg_bottom_block(Lb, V[last].x, V[last].f, bscr, rel, maxiter, nub, nuf,
+                            (int*)nullptr, sh);
     }
     // ascend
     for (int l = last - 1; l >= lc; --l)
@@ -2061,11 +2239,13 @@ __global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3(MGCoarse<T> C, T rel
         const GridDev& gc = C.op[l + 1].g;
         const int n = (int)L.g.ncell();
         const int ncx = gc.n[0], ncy = gc.n[1];
-        for (int c = threadIdx.x; c < n; c += MGC_THREADS)
+        const int nx = L.g.n[0], ny = L.g.n[1];
+        const MGCLevel<T> Vf = V[l], Vc = V[l + 1];
+        for (int m = threadIdx.x; m < n; m += MGC_THREADS)
         {
-            const int cr = V[l].crd[c];
-            const int i = cr & 1023, j = (cr >> 10) & 1023, k = cr >> 20;
-            V[l].x[c] += V[l + 1].x[(i >> 1) + ncx * ((j >> 1) + ncy * (k >> 1))];
+            const int cr = Vf.crd[m];
+            const int i = cr & 1023, j = (cr >> 10) & 1023, k = (cr >> 20) & 1023;
+            Vf.x[i + nx * (j + ny * k)] += Vc.x[(i >> 1) + ncx * ((j >> 1) + ncy * (k >> 1))];
         }
         __syncthreads();
         mgc_smooth<T, VARB>(L, V[l], nu2);
@@ -2073,10 +2253,12 @@ __global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3(MGCoarse<T> C, T rel
     {
         const MGOp<T>& L = C.op[lc];
         const int n = (int)L.g.ncell();
-        for (int c = threadIdx.x; c < n; c += MGC_THREADS)
+        const int nx = L.g.n[0], ny = L.g.n[1];
+        for (int m = threadIdx.x; m < n; m += MGC_THREADS)
         {
-            const int cr = V[lc].crd[c];
-            C.x[lc][L.g.idx(cr & 1023, (cr >> 10) & 1023, cr >> 20)] = V[lc].x[c];
+            const int cr = V[lc].crd[m];
+            const int i = cr & 1023, j = (cr >> 10) & 1023, k = (cr >> 20) & 1023;
+            C.x[lc][L.g.idx(i, j, k)] = V[lc].x[i + nx * (j + ny * k)];
         }
     }
 }
