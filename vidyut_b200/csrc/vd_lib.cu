@@ -25,6 +25,7 @@
 #include <cstring>
 #include <sstream>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace vd {
@@ -302,12 +303,38 @@ dim3 mg3_grid(const GridDev& g)
     return dim3((g.n[0] / 2 + 31) / 32, (g.n[1] + 7) / 8, (g.n[2] + MG3_U - 1) / MG3_U);
 }
 
+// Convergence check fused into the first sweep of a V-cycle (FP64 plain
+// solves): the sweep's per-block residual maxima go to part, then one block
+// reduces them into dmg->rbits and k_mg_check applies the stopping test.
+struct NormFuse
+{
+    double* part;
+    long long npart;
+    MGDev* dmg;
+    double target;
+};
+
+// Whether the first colour-0 sweep of op's level can carry the convergence
+// norm (the pair kernel with enough per-block slots).
+template <typename T>
+bool norm_fusable(const MGOp<T>& op, long long npart)
+{
+    if (!std::is_same<T, double>::value || !mg3_ok(op) || op.g.n[0] % 4) return false;
+    const bool two = op.g.ncell() >= (op.big_cells > 0 ? op.big_cells : (8LL << 20));
+    const int uv = two ? 2 : 1;
+    const long long nb = (long long)((op.g.n[0] / 2 + 63) / 64) * ((op.g.n[1] + 7) / 8) *
+                         ((op.g.n[2] + uv - 1) / uv);
+    return nb <= npart;
+}
+
 // n Gauss-Seidel iterations (colour 0, colour 1).  With xc given (only for
 // mg3_ok levels) the first colour-0 sweep also adds the prolongated coarse
-// correction xc of level gc.
+// correction xc of level gc; with nf given (norm_fusable levels) it also
+// takes the convergence norm of the current x (NormFuse).
 template <typename T>
 void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t st,
-            int prof_tag = VD_PROF_NONE, const GridDev* gc = nullptr, const T* xc = nullptr)
+            int prof_tag = VD_PROF_NONE, const GridDev* gc = nullptr, const T* xc = nullptr,
+            const NormFuse* nf = nullptr)
 {
     const long long half = (long long)((op.g.n[0] + 1) / 2) * op.g.n[1] * op.g.n[2];
     const bool prof = t_prof && prof_tag != VD_PROF_NONE && t_prof->id == prof_tag;
@@ -319,7 +346,9 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
     for (int s = 0; s < n; ++s)
         for (int color = 0; color < 2; ++color)
         {
-            if (prof) t_prof->begin(st);
+            const bool fuse = nf && s == 0 && color == 0;
+            const bool pf = prof && !fuse; // the timed sweeps are the plain ones
+            if (pf) t_prof->begin(st);
             T gamma = op.aconst; // interior diagonal of the constant-coefficient operator
             for (int d = 0; d < op.g.dim; ++d) gamma += op.dh[d] * (op.bconst + op.bconst);
             if (mg3_ok(op))
@@ -336,8 +365,22 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                     const dim3 gv((op.g.n[0] / 2 + 63) / 64, grid.y, (op.g.n[2] + uv - 1) / uv);
                     const T ig = op.b[0] ? T(0) : T(1) / gamma;
 #define VD_SWEEP3V(VB, PR, UV)                                                                \
-    LAUNCH_PDL((k_mg_sweep3v<T, VB, PR, UV>), gv, 256, st, op, x, f, color, inh ? 1 : 0, ig, gcv, xc)
-                    if (op.b[0] && pro)
+    LAUNCH_PDL((k_mg_sweep3v<T, VB, PR, UV>), gv, 256, st, op, x, f, color, inh ? 1 : 0, ig, gcv, \
+               xc, (double*)nullptr)
+#define VD_SWEEP3N(VB, UV)                                                                    \
+    LAUNCH_PDL((k_mg_sweep3v<T, VB, false, UV, true>), gv, 256, st, op, x, f, color,          \
+               inh ? 1 : 0, ig, gcv, xc, nf->part)
+                    if (fuse)
+                    {
+                        if (op.b[0])
+                            { if (two) VD_SWEEP3N(true, 2); else VD_SWEEP3N(true, 1); }
+                        else
+                            { if (two) VD_SWEEP3N(false, 2); else VD_SWEEP3N(false, 1); }
+                        const long long nbv = (long long)gv.x * gv.y * gv.z;
+                        LAUNCH_PDL(k_mg_max_partials<T>, 1, 1024, st, op, nf->part, nbv, 0,
+                                   &nf->dmg->rbits);
+                        LAUNCH_PDL(k_mg_check, 1, 1, st, nf->dmg, nf->target);
+                    } else if (op.b[0] && pro)
                         { if (two) VD_SWEEP3V(true, true, 2); else VD_SWEEP3V(true, true, 1); }
                     else if (op.b[0])
                         { if (two) VD_SWEEP3V(true, false, 2); else VD_SWEEP3V(true, false, 1); }
@@ -346,6 +389,7 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                     else
                         { if (two) VD_SWEEP3V(false, false, 2); else VD_SWEEP3V(false, false, 1); }
 #undef VD_SWEEP3V
+#undef VD_SWEEP3N
                 } else if (op.b[0])
                 {
                     if (pro)
@@ -389,7 +433,7 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                            inh ? 1 : 0, T(1) / gamma);
             } else
                 LAUNCH_PDL(k_mg_smooth_color<T>, gsz(half), BS, st, op, x, f, color, inh ? 1 : 0);
-            if (prof) t_prof->end(st);
+            if (pf) t_prof->end(st);
         }
 }
 
@@ -422,8 +466,11 @@ void bottom(Hier<T>& H, const MGOp<T>& op, T* x, const T* f, cudaStream_t st)
 // One V-cycle on level-0 unknown x0 with right-hand side f0; the level-0
 // boundary data is inhomogeneous when `inh0` (the solution itself is
 // smoothed), homogeneous otherwise (a correction is smoothed).
+// One V-cycle on x0.  With nf given, its first level-0 sweep also takes the
+// convergence norm of x0 as it was on entry (NormFuse).
 template <typename T>
-void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaStream_t st)
+void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaStream_t st,
+            const NormFuse* nf = nullptr)
 {
     const int L = H.nlev;
     if (L == 1)
@@ -444,7 +491,8 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         T* xl = l ? H.x[l] : x0;
         T* fl = l ? H.f[l] : f0;
         const bool inh = (l == 0) && inh0;
-        smooth(H.op[l], xl, fl, inh, H.nu1, st, l == 0 ? H.prof_tag : VD_PROF_NONE);
+        smooth(H.op[l], xl, fl, inh, H.nu1, st, l == 0 ? H.prof_tag : VD_PROF_NONE,
+               (const GridDev*)nullptr, (const T*)nullptr, l == 0 ? nf : nullptr);
         if (mg3_ok(H.op[l]))
         {
             const GridDev& gc = H.g[l + 1];
@@ -870,25 +918,44 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
             VD_CUDA_OK(cudaMemsetAsync(c.dmg, 0, sizeof(MGDev), c.st));
             for (auto& o : H64.op) o.stop = &c.dmg->done;
             MGOp<double> op0 = H64.op[0];
+            // the norm of cycle v's result is taken by the first sweep of
+            // cycle v+1 (NormFuse): the check lags one cycle, and a converged
+            // solution carries one more colour-0 half-sweep than the cycles
+            // counted
+            const bool fused = H64.nlev > 1 && H64.nu1 >= 1 && H64.nu2 >= 1 &&
+                               norm_fusable(op0, c.npart);
+            const NormFuse nf{c.dpart, c.npart, c.dmg, target};
             int issued = 0;
-            int batch = std::max(1, hint - 1);
+            int batch = fused ? hint + 1 : std::max(1, hint - 1);
             while (issued < cfg.linsolve_maxiter)
             {
                 const int nb = std::min(batch, cfg.linsolve_maxiter - issued);
                 for (int b = 0; b < nb; ++b)
                 {
-                    vcycle(H64, sol, rhs, true, c.dscal, c.st);
-                    // the cycle ends with a colour-1 sweep of level 0, whose
-                    // cells then have no residual: only colour 0 is scanned
-                    launch_norm(c, op0, (const double*)sol, (const double*)rhs, (double*)nullptr,
-                                true, false, &c.dmg->rbits, H64.nu2 < 1);
-                    LAUNCH_PDL(k_mg_check, 1, 1, c.st, c.dmg, target);
+                    vcycle(H64, sol, rhs, true, c.dscal, c.st, (fused && issued > 0) ? &nf : nullptr);
+                    if (!fused)
+                    {
+                        // the cycle ends with a colour-1 sweep of level 0, whose
+                        // cells then have no residual: only colour 0 is scanned
+                        launch_norm(c, op0, (const double*)sol, (const double*)rhs,
+                                    (double*)nullptr, true, false, &c.dmg->rbits, H64.nu2 < 1);
+                        LAUNCH_PDL(k_mg_check, 1, 1, c.st, c.dmg, target);
+                    }
                     ++issued;
                 }
                 VD_CUDA_OK(cudaMemcpyAsync(c.hmg, c.dmg, sizeof(MGDev), cudaMemcpyDeviceToHost, c.st));
                 VD_CUDA_OK(cudaStreamSynchronize(c.st));
                 if (c.hmg->done) break;
                 batch = 2;
+            }
+            if (fused && !c.hmg->done)
+            {
+                // the last cycle's result has not been checked yet
+                launch_norm(c, op0, (const double*)sol, (const double*)rhs, (double*)nullptr, true,
+                            false, &c.dmg->rbits, false);
+                LAUNCH_PDL(k_mg_check, 1, 1, c.st, c.dmg, target);
+                VD_CUDA_OK(cudaMemcpyAsync(c.hmg, c.dmg, sizeof(MGDev), cudaMemcpyDeviceToHost, c.st));
+                VD_CUDA_OK(cudaStreamSynchronize(c.st));
             }
             for (auto& o : H64.op) o.stop = nullptr;
             st.iterations = c.hmg->iters;

@@ -715,14 +715,25 @@ __device__ __forceinline__ T mg3_gs_value(const MGOp<T>& L, int i, int j, int k,
 // per thread (2 on the finest levels, 1 on smaller ones, where more CTAs
 // matter more: measured); warps with a row or plane on the level boundary
 // update their cells one by one with the ghost closure.
-template <typename T, bool VARB, bool PROL, int MG3_UV>
+//
+// NORM (a colour-0 sweep that starts a V-cycle): the kernel also forms the
+// residual f - L(x) of each cell it updates from the values it already holds
+// (the neighbours, f, and the cell's previous value, one more load), i.e.
+// the colour-0 residual of the previous cycle's result, and writes the
+// per-block max |r| to part[] -- the convergence norm of that cycle without a
+// pass of its own (the colour-1 residuals are zero after the previous
+// cycle's last sweep).  Same mg3_residual arithmetic as k_mg_resid3v.
+template <typename T, bool VARB, bool PROL, int MG3_UV, bool NORM = false>
 __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ MGOp<T> L,
                                                        T* __restrict__ x,
                                                        const T* __restrict__ f, int color,
                                                        int inhomog, T inv_gamma, GridDev gc,
-                                                       const T* __restrict__ xc)
+                                                       const T* __restrict__ xc,
+                                                       double* __restrict__ part)
 {
     VD_PDL_WAIT();
+    __shared__ double shm[NORM ? 32 : 1];
+    double mres = 0.0;
     using V2 = typename Vec2<T>::type;
     // the stop flag only changes between kernels: a read-only (cached) load
     const int stop = L.stop ? __ldg(L.stop) : 0;
@@ -738,12 +749,13 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
     const T* __restrict__ xo = x + (1 - color) * half;
     const T* __restrict__ fs = f + color * half;
     const bool edge = active && (j == 0 || j == ny - 1 || k0 == 0 || k0 + MG3_UV > nz - 1);
-    if (!__any_sync(0xffffffffu, edge))
+    const bool fastw = !__any_sync(0xffffffffu, edge);
+    if (fastw && active)
     {
-        if (!active) return;
         const int plane = nxh * ny;
         const int hb = 2 * pr + nxh * (j + ny * k0);
         V2 vx[MG3_UV], vym[MG3_UV], vyp[MG3_UV], vzm[MG3_UV], vzp[MG3_UV], vf[MG3_UV];
+        V2 v0[NORM ? MG3_UV : 1];
         T sx[MG3_UV];
 #pragma unroll
         for (int u = 0; u < MG3_UV; ++u)
@@ -761,6 +773,7 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
             vzm[u] = __ldg(reinterpret_cast<const V2*>(xo + h - plane));
             vzp[u] = __ldg(reinterpret_cast<const V2*>(xo + h + plane));
             vf[u] = __ldg(reinterpret_cast<const V2*>(fs + h));
+            if (NORM) v0[u] = __ldg(reinterpret_cast<const V2*>(xs + h));
         }
         // prolongation on the fly: an other-colour neighbour at half-index
         // h' of row j has coarse column h'; cells A, B (coarse columns 2pr,
@@ -845,17 +858,32 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
             nA[5] = vzp[u].x;
             nB[5] = vzp[u].y;
             const int oA = (iA == 0) ? 1 : 0, oB = (iB == nx - 1) ? 2 : 0;
+            if (NORM)
+            {
+                T rA[6], rB[6], bA[6], bB[6];
+#pragma unroll
+                for (int m = 0; m < 6; ++m)
+                {
+                    rA[m] = nA[m];
+                    rB[m] = nB[m];
+                }
+                mg3_faces<T, VARB>(L, iA, j, k, bA);
+                mg3_faces<T, VARB>(L, iB, j, k, bB);
+                const double ra = fabs((double)mg3_residual(L, vf[u].x, v0[u].x, rA, bA, oA, iA,
+                                                            j, k, inhomog != 0));
+                const double rb = fabs((double)mg3_residual(L, vf[u].y, v0[u].y, rB, bB, oB, iB,
+                                                            j, k, inhomog != 0));
+                mres = fmax(mres, fmax(ra, rb));
+            }
             V2 o;
             o.x = mg3_gs_value<T, VARB>(L, iA, j, k, oA, inhomog != 0, inv_gamma, vf[u].x, nA);
             o.y = mg3_gs_value<T, VARB>(L, iB, j, k, oB, inhomog != 0, inv_gamma, vf[u].y, nB);
             if (!stop) *reinterpret_cast<V2*>(xs + hb + u * plane) = o;
         }
-        return;
     }
-    if (!active) return;
     // boundary rows and planes: cell by cell
 #pragma unroll 1
-    for (int u = 0; u < MG3_UV; ++u)
+    for (int u = 0; u < ((!fastw && active) ? MG3_UV : 0); ++u)
     {
         const int k = k0 + u;
         if (k >= nz) break;
@@ -881,10 +909,26 @@ __global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ M
                     nb[m] += __ldg(xc + gc.idx(ci[mm] >> 1, cj[mm] >> 1, ck[mm] >> 1));
                 }
             }
-            const T v = mg3_gs_value<T, VARB>(L, i, j, k, out, inhomog != 0, inv_gamma,
-                                              __ldg(fs + h), nb);
+            const T fv = __ldg(fs + h);
+            if (NORM)
+            {
+                T rn[6], b[6];
+#pragma unroll
+                for (int m = 0; m < 6; ++m) rn[m] = nb[m];
+                mg3_faces<T, VARB>(L, i, j, k, b);
+                mres = fmax(mres, fabs((double)mg3_residual(L, fv, __ldg(xs + h), rn, b, out, i,
+                                                            j, k, inhomog != 0)));
+            }
+            const T v = mg3_gs_value<T, VARB>(L, i, j, k, out, inhomog != 0, inv_gamma, fv, nb);
             if (!stop) xs[h] = v;
         }
+    }
+    if (NORM)
+    {
+        mres = block_max(mres, shm);
+        if (threadIdx.x == 0)
+            part[blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] =
+                mres;
     }
 }
 
