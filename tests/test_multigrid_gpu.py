@@ -7,6 +7,8 @@ The FP64 solves converge to 1e-13 of the right-hand-side norm on both sides,
 so the potentials agree to 1e-11 (the comparator's relative RMS,
 py_utils/compare_fields_from_twoplotfiles.py:40-46) with V-cycle counts
 within one of each other."""
+import ctypes
+
 import pytest
 
 import vidyut_b200 as vb
@@ -166,3 +168,21 @@ def test_fp32_refined_hbm_level_sweeps(require_gpu, monkeypatch):
     assert sg.converged and so.converged
     pid = g.info["pot_id"]
     assert rel(g.get_state(pid, 1), o.get_state(pid, 1)) < 1e-9
+
+
+@pytest.mark.parametrize("maxiter", [1, 3])
+def test_poisson_stops_at_maxiter(require_gpu, maxiter):
+    """A solve cut off by linsolve_maxiter: the convergence norm of each cycle
+    is taken by the next cycle's first sweep, and the last cycle's by a
+    standalone pass, so the result is exactly `maxiter` V-cycles, as in the
+    oracle, and is reported as not converged."""
+    cfg = box(64, 64, 64, linsolve_maxiter=maxiter)
+    g, o = pair(cfg, 24)
+    sg = vb.vd_solve_stats()
+    assert vb.STATUS[g.lib.vd_poisson_solve(g.ctx, 0.0, ctypes.byref(sg))] == "VD_ERR_NOT_CONVERGED"
+    so = o.solve_potential(0.0)
+    assert not sg.converged and not so.converged
+    assert sg.iterations == so.iterations == maxiter
+    assert abs(sg.final_residual - so.final_residual) <= 1e-9 * so.final_residual
+    pid = g.info["pot_id"]
+    assert rel(g.get_state(pid, 1), o.get_state(pid, 1)) < 1e-12
