@@ -60,8 +60,21 @@ typedef struct vd_config {
     int is_periodic[3];
 
     /* time stepping: Source/TimeStep.cpp:14-43, Source/Evolve.cpp:214-617 */
-    double dt;
+    double dt;               /* the fixed step (the reference's fixed_dt)  */
     int num_timestep_correctors;
+    /* adaptive step (Source/TimeStep.cpp:14-134, Source/Vidyut.cpp:388-398):
+       with adaptive_dt and time > adaptive_dt_delay each step takes
+       min(dt_prev * dt_stretch, clamp(min(advective_cfl dt_edrift,
+       diffusive_cfl dt_ediff, dielectric_cfl dt_diel_relax), dt_min,
+       dt_max)) from the electron time scales of the state it starts from */
+    int adaptive_dt;
+    double advective_cfl;
+    double diffusive_cfl;
+    double dielectric_cfl;
+    double dt_min;
+    double dt_max;
+    double adaptive_dt_delay;
+    double dt_stretch;
 
     /* drift flux: Source/compute_explicit_flux.H:218-415 */
     int hyp_order;           /* 1 upwind, 2 WAF/MINBEE, 5 WENO5            */
@@ -157,6 +170,10 @@ typedef struct vd_step_stats {
     double time;             /* simulation time after the last step        */
     double gpu_ms;           /* device time of the steps (CUDA events on
                                 the context's stream)                     */
+    double dt;               /* step size of the last step                 */
+    double dt_edrift;        /* electron time scales of the last step's    */
+    double dt_ediff;         /* starting state (adaptive_dt only; DBL_MAX  */
+    double dt_diel_relax;    /* where undefined): Source/TimeStep.cpp:46-134 */
 } vd_step_stats;
 
 /* Kernels that vd_profile_kernel can time launch by launch. */

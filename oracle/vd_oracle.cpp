@@ -35,6 +35,7 @@
 // known-answer tests (MMS1 steady state, Advect WENO5 convergence) through
 // tests/test_oracle_known_answers.py; iteration-level agreement with MLMG
 // is unpinned because AMReX is not available to run here.
+#include <cfloat>
 #include <vidyut_b200.h>
 
 #include "vd_vars.H"
@@ -816,6 +817,8 @@ struct OCtx
     std::vector<int> bg;
     std::string err;
     long long n_poisson_iters = 0, n_species_iters = 0;
+    double fixed_dt = 0.0;                 // the configured step (fixed_dt)
+    double tscale[3] = {DBL_MAX, DBL_MAX, DBL_MAX};
 };
 
 namespace {
@@ -1408,9 +1411,66 @@ const int* bc_hi_for(const OCtx& c, int sp)
     return plasmachem::get_charge(sp) != 0 ? c.cfg.ion_bc_hi : c.cfg.neutral_bc_hi;
 }
 
+// --- Vidyut::find_time_scales (Source/TimeStep.cpp:46-134) and
+// Vidyut::ComputeDt (Source/TimeStep.cpp:14-43): electron drift,
+// diffusion and dielectric-relaxation time scales from the max-norms of
+// |mu_e||E|, D_e and |mu_e| n_e over the cells, then the adaptive step.
+void compute_dt(OCtx& c)
+{
+    const Geom& geo = c.geo;
+    const vd_config& cfg = c.cfg;
+    const Real Tg = cfg.gas_temperature;
+    const int e = c.E_IDX;
+    Real max_edriftvel = 0.0, max_ediff = 0.0, max_muene = 0.0;
+    for (int k = 0; k < geo.n[2]; ++k)
+        for (int j = 0; j < geo.n[1]; ++j)
+            for (int i = 0; i < geo.n[0]; ++i)
+            {
+                const Real etemp = c.phi_new(i, j, k, ETEMP_ID);
+                Real Esum = 0.0;
+                for (int d = 0; d < geo.dim; ++d)
+                {
+                    const Real ef = c.phi_new(i, j, k, EFX_ID + d);
+                    Esum += ef * ef;
+                }
+                const Real emag = std::sqrt(Esum);
+                Real nd = 0.0;
+                for (int sp = 0; sp < NUM_SPECIES; sp++) nd += c.phi_new(i, j, k, sp);
+                const Real dco = specDiff(e, etemp, nd, emag, Tg);
+                const Real mu = specMob(e, etemp, nd, emag, Tg);
+                max_edriftvel = std::max(max_edriftvel, std::fabs(std::fabs(mu) * emag));
+                max_ediff = std::max(max_ediff, std::fabs(dco));
+                max_muene = std::max(max_muene, std::fabs(std::fabs(mu) * c.phi_new(i, j, k, e)));
+            }
+    const Real big = DBL_MAX;
+    Real dt_edrift = big, dt_ediff = big, dt_diel_relax = big;
+    if (max_edriftvel > 0)
+        for (int d = 0; d < geo.dim; ++d) dt_edrift = std::min(dt_edrift, geo.dx[d] / max_edriftvel);
+    if (max_ediff > 0)
+        for (int d = 0; d < geo.dim; ++d)
+            dt_ediff = std::min(dt_ediff, 0.5 * geo.dx[d] * geo.dx[d] / max_ediff / geo.dim);
+    if (max_muene > 0) dt_diel_relax = EPS0 / ECHARGE / max_muene;
+    c.tscale[0] = dt_edrift;
+    c.tscale[1] = dt_ediff;
+    c.tscale[2] = dt_diel_relax;
+    if (cfg.adaptive_dt && c.cur_time > cfg.adaptive_dt_delay)
+    {
+        const Real old_dt = cfg.dt;
+        Real trans_min_dt = big;
+        if (cfg.do_transport)
+            trans_min_dt = std::min(dt_edrift * cfg.advective_cfl, dt_ediff * cfg.diffusive_cfl);
+        Real adp_dt = std::min(trans_min_dt, dt_diel_relax * cfg.dielectric_cfl);
+        if (adp_dt > cfg.dt_max) adp_dt = cfg.dt_max;
+        if (adp_dt < cfg.dt_min) adp_dt = cfg.dt_min;
+        c.cfg.dt = std::min(old_dt * cfg.dt_stretch, adp_dt);
+    } else
+        c.cfg.dt = c.fixed_dt;
+}
+
 // --- one coarse step (Source/Evolve.cpp:136-617) -------------------------
 void evolve_one(OCtx& c)
 {
+    if (c.cfg.adaptive_dt) compute_dt(c);
     const Geom& geo = c.geo;
     const Real dt = c.cfg.dt;
     c.phi_old.d = c.phi_new.d; // copy new -> old
@@ -1519,6 +1579,7 @@ int vdo_create(const vd_config* cfg, void** out)
     if (!cfg || !out) return VD_ERR_INVALID_ARG;
     auto* c = new OCtx();
     c->cfg = *cfg;
+    c->fixed_dt = cfg->dt;
     c->geo = geom_of(*cfg);
     c->ngrow = (cfg->hyp_order == 1) ? 1 : (cfg->hyp_order == 2 ? 2 : 3);
     c->phi_new.define(c->geo, NVAR, 0);
@@ -1605,6 +1666,10 @@ int vdo_step(void* ctx, int nsteps, vd_step_stats* st)
         st->poisson_iterations = (int)c->n_poisson_iters;
         st->species_iterations = (int)c->n_species_iters;
         st->time = c->cur_time;
+        st->dt = c->cfg.dt;
+        st->dt_edrift = c->tscale[0];
+        st->dt_ediff = c->tscale[1];
+        st->dt_diel_relax = c->tscale[2];
     }
     return VD_OK;
 }

@@ -40,6 +40,9 @@ class vd_config(C.Structure):
     _fields_ = [
         ("dim", C.c_int), ("n_cell", _I3), ("prob_lo", _D3), ("prob_hi", _D3),
         ("is_periodic", _I3), ("dt", C.c_double), ("num_timestep_correctors", C.c_int),
+        ("adaptive_dt", C.c_int), ("advective_cfl", C.c_double), ("diffusive_cfl", C.c_double),
+        ("dielectric_cfl", C.c_double), ("dt_min", C.c_double), ("dt_max", C.c_double),
+        ("adaptive_dt_delay", C.c_double), ("dt_stretch", C.c_double),
         ("hyp_order", C.c_int), ("weno_scheme", C.c_int),
         ("do_reactions", C.c_int), ("do_transport", C.c_int), ("do_spacechrg", C.c_int),
         ("elecenergy_solve", C.c_int), ("using_LFA", C.c_int), ("floor_jh", C.c_int),
@@ -87,7 +90,8 @@ class vd_step_stats(C.Structure):
     _fields_ = [("steps", C.c_int), ("poisson_iterations", C.c_int),
                 ("species_iterations", C.c_int), ("not_converged", C.c_int),
                 ("max_poisson_final_residual", C.c_double), ("time", C.c_double),
-                ("gpu_ms", C.c_double)]
+                ("gpu_ms", C.c_double), ("dt", C.c_double), ("dt_edrift", C.c_double),
+                ("dt_ediff", C.c_double), ("dt_diel_relax", C.c_double)]
 
 
 EXPORTS = [

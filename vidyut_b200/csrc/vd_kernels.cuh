@@ -657,6 +657,65 @@ __device__ __forceinline__ double cell_diff(const double* __restrict__ S, const 
     return specDiff(spec, S[ETEMP_ID * N + q], nd, emag, Tg);
 }
 
+// Electron time scales (find_time_scales, Source/TimeStep.cpp:46-134): the
+// max-norms of |mu_e| |E|, D_e and |mu_e| n_e over the cells, per block into
+// part[3 b + q]; k_time_scales_final reduces them into out[0..2].
+__global__ void __launch_bounds__(256) k_time_scales(GridDev g, const double* __restrict__ S,
+                                                     int eidx, double Tg,
+                                                     double* __restrict__ part)
+{
+    VD_PDL_WAIT();
+    __shared__ double sh[32];
+    const long long N = g.ncell();
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        const double etemp = S[ETEMP_ID * N + t];
+        double Esum = 0.0;
+        for (int d = 0; d < g.dim; ++d)
+        {
+            const double e = S[(EFX_ID + d) * N + t];
+            Esum += e * e;
+        }
+        const double emag = sqrt(Esum);
+        double nd = 0.0;
+#pragma unroll
+        for (int sp = 0; sp < NUM_SPECIES; sp++) nd += S[sp * N + t];
+        const double dco = specDiff(eidx, etemp, nd, emag, Tg);
+        const double mu = specMob(eidx, etemp, nd, emag, Tg);
+        m0 = fmax(m0, fabs(fabs(mu) * emag));
+        m1 = fmax(m1, fabs(dco));
+        m2 = fmax(m2, fabs(fabs(mu) * S[eidx * N + t]));
+    }
+    m0 = block_max(m0, sh);
+    m1 = block_max(m1, sh);
+    m2 = block_max(m2, sh);
+    if (threadIdx.x == 0)
+    {
+        part[3 * blockIdx.x] = m0;
+        part[3 * blockIdx.x + 1] = m1;
+        part[3 * blockIdx.x + 2] = m2;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_time_scales_final(const double* __restrict__ part,
+                                                           int nb, double* __restrict__ out)
+{
+    VD_PDL_WAIT();
+    __shared__ double sh[32];
+    double m[3] = {0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) m[q] = fmax(m[q], part[3 * b + q]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+    {
+        const double v = block_max(m[q], sh);
+        if (threadIdx.x == 0) out[q] = v;
+    }
+}
+
 // Harmonic face average of the cell diffusivity (0 where both cells are 0).
 __global__ void k_species_faces(GridDev g, int d, const double* __restrict__ S, int spec,
                                 double Tg, double* __restrict__ bf)

@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <sstream>
 #include <string>
 #include <type_traits>
@@ -612,6 +613,10 @@ struct Ctx
     int hint[VD_NT + 1] = {}; // last V-cycle count per solve (index VD_NT: Poisson)
     double time = 0.0;
     int step = 0;
+    double fixed_dt = 0.0;   // the configured step; cfg.dt is the current one
+    double* dts = nullptr;   // electron time-scale maxima (device)
+    double* hts = nullptr;   // pinned host mirror
+    double tscale[3] = {};   // time scales of the last adaptive step
     int eidx = E_ID;
     int bg[NUM_SPECIES] = {};
     int pbct[6] = {}, ebct[6] = {}, eebct[6] = {}, ibct[6] = {}, nbct[6] = {};
@@ -1166,8 +1171,47 @@ void add_solved(Ctx& c, FinalParams& P, int comp)
 }
 
 // ---- one coarse step (Source/Evolve.cpp:136-617)
+// ---- find_time_scales + ComputeDt (Source/TimeStep.cpp:14-134): the
+// electron drift, diffusion and dielectric-relaxation time scales of the
+// current state, and the step size they give.  Sets c.cfg.dt.
+void compute_dt(Ctx& c)
+{
+    const vd_config& cfg = c.cfg;
+    const double big = std::numeric_limits<double>::max();
+    const int nb = (int)std::min<long long>((c.N + 255) / 256, 4 * 148);
+    LAUNCH(k_time_scales, nb, 256, c.st, c.g, (const double*)c.S, c.eidx, cfg.gas_temperature,
+           c.dpart);
+    LAUNCH(k_time_scales_final, 1, 256, c.st, (const double*)c.dpart, nb, c.dts);
+    VD_CUDA_OK(cudaMemcpyAsync(c.hts, c.dts, 3 * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    VD_CUDA_OK(cudaStreamSynchronize(c.st));
+    const double max_edriftvel = c.hts[0], max_ediff = c.hts[1], max_muene = c.hts[2];
+    double dt_edrift = big, dt_ediff = big, dt_diel_relax = big;
+    if (max_edriftvel > 0)
+        for (int d = 0; d < cfg.dim; ++d) dt_edrift = std::min(dt_edrift, c.G.dx[d] / max_edriftvel);
+    if (max_ediff > 0)
+        for (int d = 0; d < cfg.dim; ++d)
+            dt_ediff = std::min(dt_ediff, 0.5 * c.G.dx[d] * c.G.dx[d] / max_ediff / cfg.dim);
+    if (max_muene > 0) dt_diel_relax = EPS0 / ECHARGE / max_muene;
+    c.tscale[0] = dt_edrift;
+    c.tscale[1] = dt_ediff;
+    c.tscale[2] = dt_diel_relax;
+    if (cfg.adaptive_dt && c.time > cfg.adaptive_dt_delay)
+    {
+        const double old_dt = cfg.dt;
+        double trans_min_dt = big;
+        if (cfg.do_transport)
+            trans_min_dt = std::min(dt_edrift * cfg.advective_cfl, dt_ediff * cfg.diffusive_cfl);
+        double adp_dt = std::min(trans_min_dt, dt_diel_relax * cfg.dielectric_cfl);
+        if (adp_dt > cfg.dt_max) adp_dt = cfg.dt_max;
+        if (adp_dt < cfg.dt_min) adp_dt = cfg.dt_min;
+        c.cfg.dt = std::min(old_dt * cfg.dt_stretch, adp_dt);
+    } else
+        c.cfg.dt = c.fixed_dt;
+}
+
 void step_once(Ctx& c)
 {
+    if (c.cfg.adaptive_dt) compute_dt(c);
     const vd_config& cfg = c.cfg;
     const double dt = cfg.dt;
     const int ncorr = std::max(1, cfg.num_timestep_correctors);
@@ -1248,6 +1292,10 @@ const Key g_keys[] = {
     KI3("amr.n_cell", n_cell), KD3("geometry.prob_lo", prob_lo), KD3("geometry.prob_hi", prob_hi),
     KI3("geometry.is_periodic", is_periodic), KD("vidyut.dt", dt),
     KI("vidyut.num_timestep_correctors", num_timestep_correctors),
+    KI("vidyut.adaptive_dt", adaptive_dt), KD("vidyut.advective_cfl", advective_cfl),
+    KD("vidyut.diffusive_cfl", diffusive_cfl), KD("vidyut.dielectric_cfl", dielectric_cfl),
+    KD("vidyut.dt_min", dt_min), KD("vidyut.dt_max", dt_max),
+    KD("vidyut.adaptive_dt_delay", adaptive_dt_delay), KD("vidyut.dt_stretch", dt_stretch),
     KI("vidyut.hyp_order", hyp_order), KI("vidyut.weno_scheme", weno_scheme),
     KI("vidyut.do_reactions", do_reactions), KI("vidyut.do_transport", do_transport),
     KI("vidyut.do_spacechrg", do_spacechrg), KI("vidyut.elecenergy_solve", elecenergy_solve),
@@ -1505,6 +1553,15 @@ vd_status vd_config_init(vd_config* c)
     }
     c->dt = 1e-12;
     c->num_timestep_correctors = 1;
+    // Source/Vidyut.H:251-260
+    c->adaptive_dt = 0;
+    c->advective_cfl = 0.7;
+    c->diffusive_cfl = 1.0;
+    c->dielectric_cfl = 1.0;
+    c->dt_min = 1e-14;
+    c->dt_max = 1e-9;
+    c->adaptive_dt_delay = 0.0;
+    c->dt_stretch = std::numeric_limits<double>::max();
     c->hyp_order = 1;
     c->weno_scheme = 3;
     c->do_reactions = 1;
@@ -1743,6 +1800,10 @@ vd_status vd_create(const vd_config* cfg, void** out)
         c->npart = 65536;
         c->dpart = c->A.get<double>(2 * c->npart);
         VD_CUDA_OK(cudaMallocHost(&c->hmg, sizeof(MGDev)));
+        c->fixed_dt = cfg->dt;
+        c->dts = c->A.get<double>(3);
+        VD_CUDA_OK(cudaMallocHost(&c->hts, 3 * sizeof(double)));
+        for (int q = 0; q < 3; ++q) c->tscale[q] = std::numeric_limits<double>::max();
         // electron index (Source/Vidyut.cpp:132-144)
         c->eidx = E_ID;
         VD_CUDA_OK(cudaDeviceSynchronize());
@@ -1770,6 +1831,7 @@ vd_status vd_destroy(void* ctx)
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->hscal) cudaFreeHost(c->hscal);
     if (c->hmg) cudaFreeHost(c->hmg);
+    if (c->hts) cudaFreeHost(c->hts);
     delete c->adjs;
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -1872,6 +1934,10 @@ vd_status vd_step(void* ctx, int nsteps, vd_step_stats* stats)
             stats->max_poisson_final_residual = c->max_poisson_res;
             stats->time = c->time;
             stats->gpu_ms = ms;
+            stats->dt = c->cfg.dt;
+            stats->dt_edrift = c->tscale[0];
+            stats->dt_ediff = c->tscale[1];
+            stats->dt_diel_relax = c->tscale[2];
         }
     });
     return c->not_converged ? VD_ERR_NOT_CONVERGED : VD_OK;
