@@ -213,8 +213,16 @@ vd_status vd_get_state(void* ctx, int comp, int ncomp, double* dst, int on_devic
 vd_status vd_set_time(void* ctx, double time, int step);
 vd_status vd_get_time(void* ctx, double* time, int* step);
 
+/* The current step size: the dt[] entry of a checkpoint
+ * (Vidyut::WriteCheckpointFile / ReadCheckpointFile, Source/Plot.cpp:103-108,
+ * 157-166).  It is the previous step's dt that an adaptive step stretches;
+ * without adaptive_dt every step takes the configured (fixed) dt. */
+vd_status vd_set_dt(void* ctx, double dt);
+vd_status vd_get_dt(void* ctx, double* dt);
+
 /* Advance `nsteps` coarse steps: the body of Vidyut::Evolve for one level
- * (Source/Evolve.cpp:136-617), fixed dt (Source/TimeStep.cpp:36). */
+ * (Source/Evolve.cpp:136-617), with the fixed dt or, with adaptive_dt, the
+ * step of Vidyut::ComputeDt (Source/TimeStep.cpp:14-134). */
 vd_status vd_step(void* ctx, int nsteps, vd_step_stats* stats);
 
 /* Sub-stages, each on the current state (used as both Sborder and

@@ -97,6 +97,7 @@ class vd_step_stats(C.Structure):
 EXPORTS = [
     "vd_config_init", "vd_config_set", "vd_case_info", "vd_create", "vd_destroy",
     "vd_init_domain", "vd_set_state", "vd_get_state", "vd_set_time", "vd_get_time",
+    "vd_set_dt", "vd_get_dt",
     "vd_step", "vd_poisson_solve", "vd_explicit_rhs", "vd_implicit_diffusion",
     "vd_check_state", "vd_launch_count", "vd_profile_kernel", "vd_profile_read",
     "vd_last_error", "vd_poisson_solve_noalloc", "vd_adjoint_num_params",
@@ -143,6 +144,8 @@ def load(case: str) -> C.CDLL:
         "vd_get_state": [P, C.c_int, C.c_int, P, C.c_int],
         "vd_set_time": [P, C.c_double, C.c_int],
         "vd_get_time": [P, C.POINTER(C.c_double), C.POINTER(C.c_int)],
+        "vd_set_dt": [P, C.c_double],
+        "vd_get_dt": [P, C.POINTER(C.c_double)],
         "vd_step": [P, C.c_int, C.POINTER(vd_step_stats)],
         "vd_poisson_solve": [P, C.c_double, C.POINTER(vd_solve_stats)],
         "vd_explicit_rhs": [P, C.c_double, P, C.c_int],
@@ -313,6 +316,14 @@ class Vidyut:
         self._chk(self.lib.vd_get_time(self.ctx, C.byref(t), C.byref(s)), "vd_get_time")
         return t.value, s.value
 
+    def set_dt(self, dt: float):
+        self._chk(self.lib.vd_set_dt(self.ctx, dt), "vd_set_dt")
+
+    def dt(self) -> float:
+        v = C.c_double()
+        self._chk(self.lib.vd_get_dt(self.ctx, C.byref(v)), "vd_get_dt")
+        return v.value
+
     # -- stepping and sub-stages
     def step(self, nsteps: int = 1, allow_unconverged: bool = False) -> vd_step_stats:
         st = vd_step_stats()
@@ -365,6 +376,27 @@ class Vidyut:
         t, step = self.time()
         write_plotfile(path, self.get_state(), var_names(self.info["names"]),
                        list(c.prob_lo), list(c.prob_hi), t, step, self.dim)
+
+    def write_checkpoint(self, path: str) -> None:
+        """State, step count, dt and time in the reference's checkpoint layout
+        (Vidyut::WriteCheckpointFile, Source/Plot.cpp:46-132)."""
+        from .plotfile import write_checkpoint
+        t, step = self.time()
+        write_checkpoint(path, self.get_state(), t, step, self.dt(), self.dim)
+
+    def restart(self, path: str) -> None:
+        """Continue from a checkpoint (Vidyut::ReadCheckpointFile,
+        Source/Plot.cpp:134-222): state, time, step count and dt."""
+        from .plotfile import read_checkpoint
+        ck = read_checkpoint(path)
+        data = ck["data"]
+        if data.shape[1:] != (self.shape[2], self.shape[1], self.shape[0]):
+            raise ValueError(f"checkpoint grid {data.shape[1:]} does not match the run")
+        if data.shape[0] != self.info["nvar"]:
+            raise ValueError(f"checkpoint has {data.shape[0]} components, the case {self.info['nvar']}")
+        self.set_state(0, data)
+        self.set_time(ck["time"], ck["step"])
+        self.set_dt(ck["dt"])
 
     # -- discrete adjoint of explicit flux + source steps (no reference counterpart)
     def adjoint_num_params(self) -> int:

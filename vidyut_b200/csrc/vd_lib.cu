@@ -1211,7 +1211,10 @@ void compute_dt(Ctx& c)
 
 void step_once(Ctx& c)
 {
-    if (c.cfg.adaptive_dt) compute_dt(c);
+    if (c.cfg.adaptive_dt)
+        compute_dt(c);
+    else
+        c.cfg.dt = c.fixed_dt;
     const vd_config& cfg = c.cfg;
     const double dt = cfg.dt;
     const int ncorr = std::max(1, cfg.num_timestep_correctors);
@@ -1898,6 +1901,20 @@ vd_status vd_set_time(void* ctx, double time, int step)
     Ctx* c = static_cast<Ctx*>(ctx);
     c->time = time;
     c->step = step;
+    return VD_OK;
+}
+
+vd_status vd_set_dt(void* ctx, double dt)
+{
+    if (!ctx || !(dt > 0.0)) return VD_ERR_INVALID_ARG;
+    static_cast<Ctx*>(ctx)->cfg.dt = dt;
+    return VD_OK;
+}
+
+vd_status vd_get_dt(void* ctx, double* dt)
+{
+    if (!ctx || !dt) return VD_ERR_INVALID_ARG;
+    *dt = static_cast<Ctx*>(ctx)->cfg.dt;
     return VD_OK;
 }
 
