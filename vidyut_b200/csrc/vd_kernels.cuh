@@ -293,6 +293,31 @@ __device__ __forceinline__ double grad_at_face(const GradCtx& C, const double* _
 // ---------------- E field, reduced field, potential (Source/PotentialSolve.cpp:500-541)
 // Grid: (row blocks, ny, nz).  Faces inside the domain are plain differences
 // of the solution; boundary faces go through the solve's closure.
+// E = -grad(phi) at cell (i,j,k) of the solution x0 = sol there: the mean of
+// the two face gradients, boundary faces from the solve's ghost closure.
+__device__ __forceinline__ void efield_cell(const GradCtx& C, const double* __restrict__ sol,
+                                            int i, int j, int k, double x0, double ps,
+                                            double* E)
+{
+    const GridDev& g = C.op.g;
+    const int c3[3] = {i, j, k};
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+        E[d] = 0.0;
+        if (d >= g.dim) break;
+        int m[3] = {i, j, k}, p[3] = {i, j, k};
+        m[d] -= 1;
+        p[d] += 1;
+        const double glo = (c3[d] > 0) ? (x0 - sol[g.idx(m[0], m[1], m[2])]) * C.dxi[d]
+                                       : grad_at_face(C, sol, d, i, j, k);
+        const double ghi = (c3[d] < g.n[d] - 1)
+                               ? (sol[g.idx(p[0], p[1], p[2])] - x0) * C.dxi[d]
+                               : grad_at_face(C, sol, d, p[0], p[1], p[2]);
+        E[d] = 0.5 * (glo * (-1.0 * ps) + ghi * (-1.0 * ps));
+    }
+}
+
 __global__ void __launch_bounds__(128) k_efield(GradCtx C, const double* __restrict__ sol,
                                                 double* __restrict__ S, double ps)
 {
@@ -304,23 +329,9 @@ __global__ void __launch_bounds__(128) k_efield(GradCtx C, const double* __restr
     const long long N = g.ncell();
     const long long t = i + (long long)g.n[0] * (j + (long long)g.n[1] * k);
     const double x0 = sol[g.idx(i, j, k)];
-    double E[3] = {0.0, 0.0, 0.0};
-    const int c3[3] = {i, j, k};
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-    {
-        if (d >= g.dim) break;
-        int m[3] = {i, j, k}, p[3] = {i, j, k};
-        m[d] -= 1;
-        p[d] += 1;
-        const double glo = (c3[d] > 0) ? (x0 - sol[g.idx(m[0], m[1], m[2])]) * C.dxi[d]
-                                       : grad_at_face(C, sol, d, i, j, k);
-        const double ghi = (c3[d] < g.n[d] - 1)
-                               ? (sol[g.idx(p[0], p[1], p[2])] - x0) * C.dxi[d]
-                               : grad_at_face(C, sol, d, p[0], p[1], p[2]);
-        E[d] = 0.5 * (glo * (-1.0 * ps) + ghi * (-1.0 * ps));
-        S[(EFX_ID + d) * N + t] = E[d];
-    }
+    double E[3];
+    efield_cell(C, sol, i, j, k, x0, ps, E);
+    for (int d = 0; d < g.dim; ++d) S[(EFX_ID + d) * N + t] = E[d];
     double Esum = 0.0, nd = 0.0;
 #pragma unroll
     for (int sp = 0; sp < NUM_SPECIES; sp++) nd += S[sp * N + t];
@@ -328,6 +339,48 @@ __global__ void __launch_bounds__(128) k_efield(GradCtx C, const double* __restr
     for (int d = 0; d < g.dim; ++d) Esum += E[d] * E[d];
     S[REF_ID * N + t] = (sqrt(Esum) / nd) / 1.0e-21;
     S[POT_ID * N + t] = x0 * ps;
+}
+
+// The same for two adjacent cells i, i+1 per thread (nx even): the state
+// components are read and written as 16-byte pairs.
+__global__ void __launch_bounds__(128) k_efield2(GradCtx C, const double* __restrict__ sol,
+                                                 double* __restrict__ S, double ps)
+{
+    VD_PDL_WAIT();
+    const GridDev& g = C.op.g;
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= g.n[0]) return;
+    const int j = blockIdx.y, k = blockIdx.z;
+    const long long N = g.ncell();
+    const long long t = i + (long long)g.n[0] * (j + (long long)g.n[1] * k);
+    double x0[2], E[2][3];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) x0[e] = sol[g.idx(i + e, j, k)];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) efield_cell(C, sol, i + e, j, k, x0[e], ps, E[e]);
+    for (int d = 0; d < g.dim; ++d)
+        *reinterpret_cast<double2*>(S + (EFX_ID + d) * N + t) = make_double2(E[0][d], E[1][d]);
+    double nd[2] = {0.0, 0.0};
+#pragma unroll
+    for (int sp = 0; sp < NUM_SPECIES; sp++)
+    {
+        const double2 v = *reinterpret_cast<const double2*>(S + sp * N + t);
+        nd[0] += v.x;
+        nd[1] += v.y;
+    }
+    const double2 ne = *reinterpret_cast<const double2*>(S + E_ID * N + t);
+    nd[0] = nd[0] - ne.x;
+    nd[1] = nd[1] - ne.y;
+    double r[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+    {
+        double Esum = 0.0;
+        for (int d = 0; d < g.dim; ++d) Esum += E[e][d] * E[e][d];
+        r[e] = (sqrt(Esum) / nd[e]) / 1.0e-21;
+    }
+    *reinterpret_cast<double2*>(S + REF_ID * N + t) = make_double2(r[0], r[1]);
+    *reinterpret_cast<double2*>(S + POT_ID * N + t) = make_double2(x0[0] * ps, x0[1] * ps);
 }
 
 // ---------------- fused reactions + drift flux + divergence

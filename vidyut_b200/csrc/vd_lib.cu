@@ -1008,6 +1008,12 @@ void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats)
     c.poisson_iters += it;
     c.max_poisson_res = std::max(c.max_poisson_res, st.final_residual);
     if (stats) *stats = st;
+    if (c.g.n[0] % 2 == 0)
+    {
+        // two cells per thread, 16-byte state accesses
+        const dim3 grid((c.g.n[0] / 2 + 127) / 128, c.g.n[1], c.g.n[2]);
+        LAUNCH(k_efield2, grid, 128, c.st, grad_ctx(c, c.HP, c.pside), c.phi_sol, c.S, ps);
+    } else
     {
         const Grid3 ge = rows3(c.g);
         LAUNCH(k_efield, ge.g, ge.b, c.st, grad_ctx(c, c.HP, c.pside), c.phi_sol, c.S, ps);
