@@ -67,6 +67,13 @@ typedef struct vd_config {
        min(dt_prev * dt_stretch, clamp(min(advective_cfl dt_edrift,
        diffusive_cfl dt_ediff, dielectric_cfl dt_diel_relax), dt_min,
        dt_max)) from the electron time scales of the state it starts from */
+    /* semi-implicit electron-Poisson coupling (Source/Evolve.cpp:281-352,
+       Source/PotentialSolve.cpp:262-343): the electron solve precedes the
+       potential solve, whose operator gets b = -(1 + dt/tau_diel) and whose
+       right-hand side the electron density change; repeated
+       electron_poisson_maxiters times per corrector iteration */
+    int electron_poisson_coupling;
+    int electron_poisson_maxiters;
     int adaptive_dt;
     double advective_cfl;
     double diffusive_cfl;

@@ -887,7 +887,8 @@ Real applied_potential(Real t, int domend, int vprof, Real v1, Real v2,
 
 // --- solve_potential (Source/PotentialSolve.cpp:19-554) ----------------
 void solve_potential(OCtx& c, Real time, Fab& Sborder, Fab& Sborder_old,
-                     FaceFab* efield_fc, vd_solve_stats* st)
+                     FaceFab* efield_fc, vd_solve_stats* st, int coupled = 0, Real dt = 0.0,
+                     const std::vector<Real>* ephi = nullptr)
 {
     const Geom& geo = c.geo;
     const vd_config& cfg = c.cfg;
@@ -929,8 +930,42 @@ void solve_potential(OCtx& c, Real time, Fab& Sborder, Fab& Sborder_old,
                     rhs[OMG::idx(geo, i, j, k)] = r;
                 }
     }
-    // coefficients: a = 0, b = -1 harmonic-averaged (= -1)
+    // coefficients: a = 0, b = -1 harmonic-averaged (= -1); with the
+    // electron coupling b = -(1 + dt/tau_diel) in real cells (on the grown
+    // box, ghosts from Sborder), harmonic-averaged onto the faces
+    // (Source/PotentialSolve.cpp:272-347)
     for (int d = 0; d < 3; ++d) std::fill(mg.L[0].b[d].begin(), mg.L[0].b[d].end(), -1.0);
+    if (coupled)
+    {
+        const Real Tg = cfg.gas_temperature;
+        const int e = c.E_IDX;
+        auto bcell = [&](int i, int j, int k) {
+            if (sb(i, j, k, CMASK_ID) != 1) return Real(-1.0);
+            Real Es = 0.0, nd = 0.0;
+            for (int d = 0; d < geo.dim; ++d) Es += sb(i, j, k, EFX_ID + d) * sb(i, j, k, EFX_ID + d);
+            const Real emag = std::sqrt(Es);
+            for (int sp = 0; sp < NUM_SPECIES; sp++) nd += sb(i, j, k, sp);
+            const Real mu_e = specMob(e, sb(i, j, k, ETEMP_ID), nd, emag, Tg);
+            const Real tau_diel = std::fabs(EPS0 / (ECHARGE * mu_e * sb(i, j, k, e)));
+            return -(1.0 + dt / tau_diel);
+        };
+        for (int d = 0; d < geo.dim; ++d)
+        {
+            const int nx = geo.n[0] + (d == 0), ny = geo.n[1] + (d == 1), nz = geo.n[2] + (d == 2);
+#pragma omp parallel for collapse(2)
+            for (int k = 0; k < nz; ++k)
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i)
+                    {
+                        int m[3] = {i, j, k};
+                        m[d] -= 1;
+                        const Real b0 = bcell(m[0], m[1], m[2]), b1 = bcell(i, j, k);
+                        mg.L[0].b[d][OMG::fidx(geo, d, i, j, k)] = 2.0 * b0 * b1 / (b0 + b1);
+                    }
+        }
+    }
+    if (ephi)
+        for (long long q = 0; q < N; ++q) rhs[q] = rhs[q] + (*ephi)[q];
     // boundary data via potential_bc
     BndryData bd;
     for (int s = 0; s < 6; ++s)
@@ -1493,15 +1528,46 @@ void evolve_one(OCtx& c)
         const Real t = c.cur_time + toff;
         fill_patch(geo, c.phi_new, Sborder, NVAR);
         expl.setVal(0.0);
-        solve_potential(c, t, Sborder, Sborder_old, efield, nullptr);
-        fill_patch(geo, c.phi_new, Sborder, NVAR);
-        rxn.setVal(0.0);
-        if (c.cfg.do_reactions) update_rxnsrc(c, Sborder, rxn, t);
         const int e = c.E_IDX;
-        expl.setVal(0.0);
-        update_explsrc(c, e, c.cfg.eden_bc_lo, c.cfg.eden_bc_hi, Sborder, rxn, expl, t);
-        implicit_solve(c, t, dt, e, Sborder, Sborder_old, expl, c.cfg.eden_bc_lo,
-                       c.cfg.eden_bc_hi, gradne, nullptr);
+        if (!c.cfg.electron_poisson_coupling)
+        {
+            solve_potential(c, t, Sborder, Sborder_old, efield, nullptr);
+            fill_patch(geo, c.phi_new, Sborder, NVAR);
+            rxn.setVal(0.0);
+            if (c.cfg.do_reactions) update_rxnsrc(c, Sborder, rxn, t);
+            expl.setVal(0.0);
+            update_explsrc(c, e, c.cfg.eden_bc_lo, c.cfg.eden_bc_hi, Sborder, rxn, expl, t);
+            implicit_solve(c, t, dt, e, Sborder, Sborder_old, expl, c.cfg.eden_bc_lo,
+                           c.cfg.eden_bc_hi, gradne, nullptr);
+        } else
+        {
+            // electron solve, then the potential with the electron density
+            // change (Source/Evolve.cpp:281-352)
+            const long long N = geo.ncell();
+            std::vector<Real> ephi(N);
+            for (int it = 0; it < std::max(1, c.cfg.electron_poisson_maxiters); ++it)
+            {
+                rxn.setVal(0.0);
+                if (c.cfg.do_reactions) update_rxnsrc(c, Sborder, rxn, t);
+                expl.setVal(0.0);
+                update_explsrc(c, e, c.cfg.eden_bc_lo, c.cfg.eden_bc_hi, Sborder, rxn, expl, t);
+                implicit_solve(c, t, dt, e, Sborder, Sborder_old, expl, c.cfg.eden_bc_lo,
+                               c.cfg.eden_bc_hi, gradne, nullptr);
+                // ephi = ((n_e^new - n_e^old)/dt - S_expl + S_rxn) dt e / eps0
+                for (int k = 0; k < geo.n[2]; ++k)
+                    for (int j = 0; j < geo.n[1]; ++j)
+                        for (int i = 0; i < geo.n[0]; ++i)
+                        {
+                            Real v = (1.0 / dt) * c.phi_new(i, j, k, e) +
+                                     (-1.0 / dt) * c.phi_old(i, j, k, e);
+                            v = v + (-1.0) * expl(i, j, k, e);
+                            v = v + 1.0 * rxn(i, j, k, e);
+                            ephi[OMG::idx(geo, i, j, k)] = v * (dt * ECHARGE / EPS0);
+                        }
+                solve_potential(c, t, Sborder, Sborder_old, efield, nullptr, 1, dt, &ephi);
+                fill_patch(geo, c.phi_new, Sborder, NVAR);
+            }
+        }
         if (c.cfg.elecenergy_solve)
         {
             expl.setVal(0.0);

@@ -40,6 +40,7 @@ class vd_config(C.Structure):
     _fields_ = [
         ("dim", C.c_int), ("n_cell", _I3), ("prob_lo", _D3), ("prob_hi", _D3),
         ("is_periodic", _I3), ("dt", C.c_double), ("num_timestep_correctors", C.c_int),
+        ("electron_poisson_coupling", C.c_int), ("electron_poisson_maxiters", C.c_int),
         ("adaptive_dt", C.c_int), ("advective_cfl", C.c_double), ("diffusive_cfl", C.c_double),
         ("dielectric_cfl", C.c_double), ("dt_min", C.c_double), ("dt_max", C.c_double),
         ("adaptive_dt_delay", C.c_double), ("dt_stretch", C.c_double),

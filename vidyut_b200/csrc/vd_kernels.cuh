@@ -96,7 +96,7 @@ __device__ __forceinline__ GpuArray<Real, 3> ga3(const double* v)
 __global__ void k_poisson_rhs(Geo G, GridDev gm, const double* __restrict__ Sold, double* Sv,
                               double* __restrict__ rhs, double* __restrict__ sol,
                               int do_spacechrg, int warm, double ps, double time,
-                              const ProbParm* pp)
+                              const ProbParm* pp, const double* __restrict__ ephi)
 {
     VD_PDL_WAIT();
     const long long N = G.g.ncell();
@@ -123,6 +123,7 @@ __global__ void k_poisson_rhs(Geo G, GridDev gm, const double* __restrict__ Sold
                                                      ga3(G.dx), time, *pp);
 #endif
         }
+        if (ephi) r = r + ephi[t]; // electron-Poisson coupling source
         rhs[m] = r * (1.0 / ps);
         sol[m] = warm ? Sv[POT_ID * N + t] / ps : 0.0;
     }
@@ -394,6 +395,8 @@ struct ExplParams
     const double* S;
     double* expl;
     double* rxn_een;
+    double* rxn_e; // electron reaction source (electron-Poisson coupling), or null
+    int eidx;
     double Tg, Pg, time, dt, dxmin;
     int hyp_order, weno_scheme, user_vel, do_transport, do_reactions, do_bg_rxn;
     int ntr;
@@ -640,6 +643,7 @@ __global__ void __launch_bounds__(256, EX_MINB) k_explicit_stream(ExplParams P, 
 #endif
                 }
                 if (P.rxn_een) P.rxn_een[t] = rxa[NUM_SPECIES];
+                if (P.rxn_e) P.rxn_e[t] = rxa[P.eidx];
 #pragma unroll
                 for (int sp = 0; sp < NUM_SPECIES; sp++)
                     if (P.bg[sp]) P.expl[sp * N + t] = P.do_bg_rxn ? rxa[sp] : 0.0;
@@ -766,6 +770,81 @@ __global__ void __launch_bounds__(256) k_time_scales_final(const double* __restr
     {
         const double v = block_max(m[q], sh);
         if (threadIdx.x == 0) out[q] = v;
+    }
+}
+
+// Electron-Poisson coupling (Source/PotentialSolve.cpp:272-347): the
+// potential operator's cell coefficient b = -(1 + dt/tau_diel),
+// tau_diel = |eps0 / (e mu_e n_e)| (-1 outside real cells), from the state
+// with clamped (foextrap) or wrapped neighbours, harmonic-averaged onto the
+// faces of direction d.
+__device__ __forceinline__ double pot_bcell(const double* __restrict__ S, const GridDev& g,
+                                            long long N, int eidx, int i, int j, int k,
+                                            double Tg, double dt)
+{
+    const long long q = g.idx(clampi(i, g.n[0], g.per[0]), clampi(j, g.n[1], g.per[1]),
+                              clampi(k, g.n[2], g.per[2]));
+    if (S[CMASK_ID * N + q] != 1.0) return -1.0;
+    double Es = 0.0, nd = 0.0;
+    for (int d = 0; d < g.dim; ++d)
+    {
+        const double e = S[(EFX_ID + d) * N + q];
+        Es += e * e;
+    }
+    const double emag = sqrt(Es);
+#pragma unroll
+    for (int sp = 0; sp < NUM_SPECIES; sp++) nd += S[sp * N + q];
+    const double mu_e = specMob(eidx, S[ETEMP_ID * N + q], nd, emag, Tg);
+    const double tau_diel = fabs(EPS0 / (ECHARGE * mu_e * S[eidx * N + q]));
+    return -(1.0 + dt / tau_diel);
+}
+
+__global__ void k_pot_faces(GridDev g, int d, const double* __restrict__ S, int eidx, double Tg,
+                            double dt, double* __restrict__ bf)
+{
+    VD_PDL_WAIT();
+    const long long tot = face_count(g, d);
+    const long long N = g.ncell();
+    const int nx = g.n[0] + (d == 0), ny = g.n[1] + (d == 1);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        const int i = (int)(t % nx);
+        const long long r = t / nx;
+        const int j = (int)(r % ny);
+        const int k = (int)(r / ny);
+        int m[3] = {i, j, k};
+        m[d] -= 1;
+        const double b0 = pot_bcell(S, g, N, eidx, m[0], m[1], m[2], Tg, dt);
+        const double b1 = pot_bcell(S, g, N, eidx, i, j, k, Tg, dt);
+        bf[t] = 2.0 * b0 * b1 / (b0 + b1);
+    }
+}
+
+// After the coupled electron solve: the floored electron density into the
+// state (as Vidyut::implicit_solve_scalar stores it, so the stages after it
+// read it, Source/Evolve.cpp:305-343) and the coupling source
+// ephi = ((n_e^new - n_e^old)/dt - S_expl + S_rxn) dt e / eps0.
+__global__ void k_ephi(GridDev g, GridDev gm, double* __restrict__ S,
+                       const double* __restrict__ Sold, const double* __restrict__ u,
+                       double scale, const double* __restrict__ expl,
+                       const double* __restrict__ rxn_e, int eidx, int bound, double min_e,
+                       double dt, double* __restrict__ ephi)
+{
+    VD_PDL_WAIT();
+    const long long N = g.ncell();
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        cell_of(g, t, i, j, k);
+        double ne = u[gm.idx(i, j, k)] * scale;
+        if (bound && ne < min_e) ne = min_e;
+        S[eidx * N + t] = ne;
+        double v = (1.0 / dt) * ne + (-1.0 / dt) * Sold[eidx * N + t];
+        v = v + (-1.0) * expl[eidx * N + t];
+        v = v + 1.0 * rxn_e[t];
+        ephi[t] = v * (dt * ECHARGE / EPS0);
     }
 }
 

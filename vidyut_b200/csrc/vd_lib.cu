@@ -590,7 +590,9 @@ struct Ctx
     long long N = 0;
     Alloc A;
     double* S = nullptr;
-    double* Sold = nullptr; // separate copy only with >1 corrector
+    double* Sold = nullptr; // separate copy only with >1 corrector or the coupling
+    double* rxn_e = nullptr; // electron reaction source (electron-Poisson coupling)
+    double* ephi = nullptr;  // coupling source of the potential equation
     double* expl = nullptr;
     double* rxn_een = nullptr;
     double* ejh = nullptr;
@@ -983,13 +985,28 @@ GradCtx grad_ctx(Ctx& c, Hier<double>& H, SideArrays* sides)
 }
 
 // ---- solve_potential (Source/PotentialSolve.cpp:19-554)
-void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats)
+void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats,
+             const double* ephi = nullptr)
 {
     const vd_config& cfg = c.cfg;
     const double ps = cfg.potential_scale;
     LAUNCH(k_poisson_rhs, gsz(c.N), BS, c.st, c.G, c.HP.g[0], Sold, c.S, c.phi_rhs, c.phi_sol,
-           cfg.do_spacechrg, cfg.poisson_warm_start, ps, time, c.dpp);
+           cfg.do_spacechrg, cfg.poisson_warm_start, ps, time, c.dpp, ephi);
     fill_bc(c, 0, POT_ID, c.pbct, 2, 1.0 / ps, time, c.pside);
+    if (c.HP.varb)
+    {
+        // electron-Poisson coupling: b = -(1 + dt/tau_diel) on the faces of
+        // the coupled solve, b = -1 for a plain one
+        for (int d = 0; d < cfg.dim; ++d)
+        {
+            const long long nf = face_count(c.g, d);
+            if (ephi)
+                LAUNCH(k_pot_faces, gsz(nf), BS, c.st, c.g, d, (const double*)c.S, c.eidx,
+                       cfg.gas_temperature, cfg.dt, c.HP.bf[0][d]);
+            else
+                LAUNCH(k_fill<double>, gsz(nf), BS, c.st, c.HP.bf[0][d], -1.0, nf);
+        }
+    }
     hier_set_ops(c.HP, 0.0, 1.0, -1.0, c.pbct, 2);
     hier_coarsen_coeffs(c.HP, c.pbct, c.st);
     if (cfg.mg_precision == VD_MG_FP32_REFINED)
@@ -1003,7 +1020,8 @@ void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats)
             LAUNCH(k_inneu_adjust, gsz(plane_count(c.g, s % 3)), BS, c.st, c.HP.g[0], s,
                    (const double*)nullptr, -1.0, 1.0, c.G.dx[s % 3], c.pside[s].val, c.phi_rhs);
     vd_solve_stats st{};
-    const int it = mg_solve(c, c.HP, c.HP32, c.phi_sol, c.phi_rhs, &st, c.hint[VD_NT]);
+    const int it = mg_solve(c, c.HP, c.HP32, c.phi_sol, c.phi_rhs, &st, c.hint[VD_NT],
+                            !c.HP.varb);
     if (st.converged && it > 0) c.hint[VD_NT] = it;
     c.poisson_iters += it;
     c.max_poisson_res = std::max(c.max_poisson_res, st.final_residual);
@@ -1021,7 +1039,9 @@ void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats)
 }
 
 // ---- explicit sources of every transported component
-void explicit_rhs(Ctx& c, double time)
+// Launches [qlo, qhi) of the component groups (default: all).  The first
+// launch also evaluates the chemistry of every component.
+void explicit_rhs(Ctx& c, double time, int qlo = 0, int qhi = 1 << 30)
 {
     const vd_config& cfg = c.cfg;
     ExplParams P{};
@@ -1029,6 +1049,8 @@ void explicit_rhs(Ctx& c, double time)
     P.S = c.S;
     P.expl = c.expl;
     P.rxn_een = cfg.elecenergy_solve ? c.rxn_een : nullptr;
+    P.rxn_e = c.rxn_e;
+    P.eidx = c.eidx;
     P.Tg = cfg.gas_temperature;
     P.Pg = cfg.gas_pressure;
     P.time = time;
@@ -1081,7 +1103,7 @@ void explicit_rhs(Ctx& c, double time)
     const int zc = (cfg.dim == 3) ? std::min(EX_ZC, c.g.n[2]) : 1;
     const dim3 grid((c.g.n[0] + EX_TX - 1) / EX_TX, (c.g.n[1] + EX_TY - 1) / EX_TY,
                     (c.g.n[2] + zc - 1) / zc);
-    for (int q0 = 0; q0 < std::max(n, 1); q0 += EX_QB)
+    for (int q0 = qlo * EX_QB; q0 < std::min(std::max(n, 1), qhi * EX_QB); q0 += EX_QB)
         LAUNCH(k_explicit_stream, grid, EX_TX * EX_TY, c.st, P, q0, zc);
     if (prof) t_prof->end(c.st);
 }
@@ -1225,15 +1247,36 @@ void step_once(Ctx& c)
     const double dt = cfg.dt;
     const int ncorr = std::max(1, cfg.num_timestep_correctors);
     const size_t bytes = sizeof(double) * (size_t)NVAR * c.N;
-    if (ncorr > 1) VD_CUDA_OK(cudaMemcpyAsync(c.Sold, c.S, bytes, cudaMemcpyDeviceToDevice, c.st));
-    const double* Sold = (ncorr > 1) ? c.Sold : c.S;
+    const bool own_old = ncorr > 1 || cfg.electron_poisson_coupling;
+    if (own_old) VD_CUDA_OK(cudaMemcpyAsync(c.Sold, c.S, bytes, cudaMemcpyDeviceToDevice, c.st));
+    const double* Sold = own_old ? c.Sold : c.S;
     for (int niter = 0; niter < ncorr; ++niter)
     {
         const double t = c.time + ((niter > 0) ? 0.5 * dt : 0.0);
-        poisson(c, t, Sold, nullptr);
-        explicit_rhs(c, t);
         FinalParams P = final_params(c);
-        species_solve(c, c.eidx, t, Sold, nullptr);
+        if (!cfg.electron_poisson_coupling)
+        {
+            poisson(c, t, Sold, nullptr);
+            explicit_rhs(c, t);
+            species_solve(c, c.eidx, t, Sold, nullptr);
+        } else
+        {
+            // electron solve first, then the potential with the electron
+            // density change (Source/Evolve.cpp:281-352); the electron
+            // component is the first group launch, which also evaluates the
+            // chemistry that the later launches read back
+            for (int it = 0; it < std::max(1, cfg.electron_poisson_maxiters); ++it)
+            {
+                explicit_rhs(c, t, 0, 1);
+                species_solve(c, c.eidx, t, Sold, nullptr);
+                LAUNCH(k_ephi, gsz(c.N), BS, c.st, c.g, c.HS.g[0], c.S, Sold,
+                       (const double*)c.u[c.eidx], cfg.species_scale[c.eidx],
+                       (const double*)c.expl, (const double*)c.rxn_e, c.eidx,
+                       cfg.bound_specden, cfg.min_electron_density, dt, c.ephi);
+                poisson(c, t, Sold, nullptr, c.ephi);
+            }
+            explicit_rhs(c, t, 1);
+        }
         add_solved(c, P, c.eidx);
         if (cfg.elecenergy_solve)
         {
@@ -1301,6 +1344,8 @@ const Key g_keys[] = {
     KI3("amr.n_cell", n_cell), KD3("geometry.prob_lo", prob_lo), KD3("geometry.prob_hi", prob_hi),
     KI3("geometry.is_periodic", is_periodic), KD("vidyut.dt", dt),
     KI("vidyut.num_timestep_correctors", num_timestep_correctors),
+    KI("vidyut.electron_poisson_coupling", electron_poisson_coupling),
+    KI("vidyut.electron_poisson_maxiters", electron_poisson_maxiters),
     KI("vidyut.adaptive_dt", adaptive_dt), KD("vidyut.advective_cfl", advective_cfl),
     KD("vidyut.diffusive_cfl", diffusive_cfl), KD("vidyut.dielectric_cfl", dielectric_cfl),
     KD("vidyut.dt_min", dt_min), KD("vidyut.dt_max", dt_max),
@@ -1562,7 +1607,9 @@ vd_status vd_config_init(vd_config* c)
     }
     c->dt = 1e-12;
     c->num_timestep_correctors = 1;
-    // Source/Vidyut.H:251-260
+    // Source/Vidyut.H:251-262
+    c->electron_poisson_coupling = 0;
+    c->electron_poisson_maxiters = 1;
     c->adaptive_dt = 0;
     c->advective_cfl = 0.7;
     c->diffusive_cfl = 1.0;
@@ -1702,6 +1749,32 @@ vd_status vd_create(const vd_config* cfg, void** out)
             g_create_err = "bad grid";
             return VD_ERR_INVALID_ARG;
         }
+    if (cfg->electron_poisson_coupling)
+    {
+        // the coupled step runs the electrons as the first explicit group
+        // launch (E_ID is the first transported species) and forms the
+        // potential operator from face coefficients, for which the
+        // inhomogeneous-Neumann right-hand-side adjustment is not built
+        bool first = true;
+        for (int sp = 0; sp < E_ID; ++sp)
+        {
+            bool bg = false;
+            for (int i = 0; i < cfg->num_bg_species; ++i) bg = bg || cfg->bg_species_ids[i] == sp;
+            first = first && bg;
+        }
+        for (int s = 0; s < 6; ++s)
+        {
+            const int code = (s < 3) ? cfg->pot_bc_lo[s] : cfg->pot_bc_hi[s - 3];
+            if (s % 3 < cfg->dim && code == IHNEUBC) first = false;
+        }
+        if (!first || cfg->mg_precision != VD_MG_FP64)
+        {
+            g_create_err = "electron_poisson_coupling needs the electrons as the first transported "
+                           "species, no inhomogeneous-Neumann potential boundary, and the FP64 "
+                           "multigrid form";
+            return VD_ERR_UNSUPPORTED;
+        }
+    }
     Ctx* c = new Ctx();
     try
     {
@@ -1737,7 +1810,15 @@ vd_status vd_create(const vd_config* cfg, void** out)
         const long long N = c->N;
         c->S = c->A.get<double>((size_t)NVAR * N);
         VD_CUDA_OK(cudaMemset(c->S, 0, sizeof(double) * (size_t)NVAR * N));
-        c->Sold = (cfg->num_timestep_correctors > 1) ? c->A.get<double>((size_t)NVAR * N) : c->S;
+        const bool coupled = cfg->electron_poisson_coupling != 0;
+        c->Sold = (cfg->num_timestep_correctors > 1 || coupled)
+                      ? c->A.get<double>((size_t)NVAR * N)
+                      : c->S;
+        if (coupled)
+        {
+            c->rxn_e = c->A.get<double>(N);
+            c->ephi = c->A.get<double>(N);
+        }
         c->expl = c->A.get<double>((size_t)VD_NT * N);
         VD_CUDA_OK(cudaMemset(c->expl, 0, sizeof(double) * (size_t)VD_NT * N));
         c->rxn_een = c->A.get<double>(N);
@@ -1763,7 +1844,8 @@ vd_status vd_create(const vd_config* cfg, void** out)
         }
         const double dx[3] = {c->G.dx[0], c->G.dx[1], c->G.dx[2]};
         const int mcl = cfg->linsolve_max_coarsening_level;
-        hier_build(c->HP, c->A, g, dx, mcl, false, false);
+        // the coupled potential operator has face coefficients
+        hier_build(c->HP, c->A, g, dx, mcl, coupled, false);
         hier_build(c->HS, c->A, g, dx, mcl, true, false);
         // the FP64 species hierarchy's level-0 faces are written by the set-up
         // kernels; boundary arrays of both FP64 hierarchies alias the side arrays
