@@ -467,6 +467,11 @@ void bottom(Hier<T>& H, const MGOp<T>& op, T* x, const T* f, cudaStream_t st)
 // One V-cycle on level-0 unknown x0 with right-hand side f0; the level-0
 // boundary data is inhomogeneous when `inh0` (the solution itself is
 // smoothed), homogeneous otherwise (a correction is smoothed).
+// Restriction of the colour-0 residuals only (k_mg_restrict3 C0ONLY); 0: all.
+#ifndef VD_RESTRICT_C0
+#define VD_RESTRICT_C0 1
+#endif
+
 // One V-cycle on x0.  With nf given, its first level-0 sweep also takes the
 // convergence norm of x0 as it was on entry (NormFuse).
 template <typename T>
@@ -498,12 +503,17 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         {
             const GridDev& gc = H.g[l + 1];
             const dim3 grid((gc.n[0] + 31) / 32, (gc.n[1] + 7) / 8, gc.n[2]);
+            // after pre-smoothing (last sweep colour 1) only colour 0 has a
+            // residual
+            const bool c0 = VD_RESTRICT_C0 && H.nu1 >= 1;
+#define VD_RESTRICT3(VB, C0)                                                                  \
+    LAUNCH_PDL((k_mg_restrict3<T, VB, C0>), grid, 256, st, H.op[l], xl, fl, gc, H.f[l + 1],   \
+               H.x[l + 1], inh ? 1 : 0)
             if (H.op[l].b[0])
-                LAUNCH_PDL((k_mg_restrict3<T, true>), grid, 256, st, H.op[l], xl, fl, gc,
-                       H.f[l + 1], H.x[l + 1], inh ? 1 : 0);
+                { if (c0) VD_RESTRICT3(true, true); else VD_RESTRICT3(true, false); }
             else
-                LAUNCH_PDL((k_mg_restrict3<T, false>), grid, 256, st, H.op[l], xl, fl, gc,
-                       H.f[l + 1], H.x[l + 1], inh ? 1 : 0);
+                { if (c0) VD_RESTRICT3(false, true); else VD_RESTRICT3(false, false); }
+#undef VD_RESTRICT3
             continue;
         }
         const Grid3 gr = rows3(H.g[l + 1]);
