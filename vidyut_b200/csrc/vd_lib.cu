@@ -1114,7 +1114,7 @@ void explicit_rhs(Ctx& c, double time, int qlo = 0, int qhi = 1 << 30)
     const dim3 grid((c.g.n[0] + EX_TX - 1) / EX_TX, (c.g.n[1] + EX_TY - 1) / EX_TY,
                     (c.g.n[2] + zc - 1) / zc);
     for (int q0 = qlo * EX_QB; q0 < std::min(std::max(n, 1), qhi * EX_QB); q0 += EX_QB)
-        LAUNCH(k_explicit_stream, grid, EX_TX * EX_TY, c.st, P, q0, zc);
+        LAUNCH(k_explicit_stream, grid, EX_THREADS, c.st, P, q0, zc);
     if (prof) t_prof->end(c.st);
 }
 
