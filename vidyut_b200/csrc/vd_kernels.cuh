@@ -461,7 +461,7 @@ __device__ __forceinline__ void ex_cell_vel(const ExplParams& P, int ci, int cj,
 }
 
 #ifndef EX_ZC
-#define EX_ZC 32 // planes per CTA in z (+ 6 halo planes of the z stencil)
+#define EX_ZC 0 // planes per CTA in z (0: chosen per grid, explicit_zchunk)
 #endif
 #ifndef EX_MINB
 #define EX_MINB 3 // CTAs per SM the register budget is sized for (measured: 3 beats 2)
