@@ -723,8 +723,14 @@ __device__ __forceinline__ T mg3_gs_value(const MGOp<T>& L, int i, int j, int k,
 // per-block max |r| to part[] -- the convergence norm of that cycle without a
 // pass of its own (the colour-1 residuals are zero after the previous
 // cycle's last sweep).  Same mg3_residual arithmetic as k_mg_resid3v.
+// CTAs per SM the sweep's registers are sized for: 4 (64 registers) for
+// constant coefficients; 3 for face coefficients, whose extra loads spill at
+// 64 (measured at 256^3: 0.11 ms per step less).
+#ifndef VD_SWEEP_VARB_MINB
+#define VD_SWEEP_VARB_MINB 3
+#endif
 template <typename T, bool VARB, bool PROL, int MG3_UV, bool NORM = false>
-__global__ void __launch_bounds__(256, 4) k_mg_sweep3v(const __grid_constant__ MGOp<T> L,
+__global__ void __launch_bounds__(256, VARB ? VD_SWEEP_VARB_MINB : 4) k_mg_sweep3v(const __grid_constant__ MGOp<T> L,
                                                        T* __restrict__ x,
                                                        const T* __restrict__ f, int color,
                                                        int inhomog, T inv_gamma, GridDev gc,
@@ -999,8 +1005,13 @@ __device__ __forceinline__ T mg3_residual(const MGOp<T>& L, T fv, T x0, T* nb, c
 // C0ONLY: after pre-smoothing, whose last sweep is colour 1, the colour-1
 // residuals are zero up to rounding, so only the four colour-0 children are
 // summed (reads 12 instead of 16 B/cell: no colour-1 f).
+// CTAs per SM for the restriction (measured at 256^3: 4 is 0.13 ms per step
+// faster than 3 once only the colour-0 children are read).
+#ifndef VD_RESTRICT_MINB
+#define VD_RESTRICT_MINB 4
+#endif
 template <typename T, bool VARB, bool C0ONLY = false>
-__global__ void __launch_bounds__(256, 3) k_mg_restrict3(const __grid_constant__ MGOp<T> L,
+__global__ void __launch_bounds__(256, VD_RESTRICT_MINB) k_mg_restrict3(const __grid_constant__ MGOp<T> L,
                                                       const T* __restrict__ x,
                                                       const T* __restrict__ f, GridDev gc,
                                                       T* __restrict__ fc, T* __restrict__ xc,
