@@ -321,11 +321,15 @@ vd_status vd_adjoint_run(void* ctx, int nsteps, int K, int objective_id, double*
  * Its multigrid scratch is one fixed array of 8 MiB per device, built into
  * the library and held by every device that loads it until the process
  * exits; grids needing more (above about 128^3 cells) are rejected with
- * VD_ERR_INVALID_ARG and a message saying how much they need.  The first
- * call on a device looks up that array's device address (with the device
- * current), so make that first call before any stream capture.  Work runs on
- * the legacy default stream; every call reuses the same scratch, so calls
- * that overlap on one device race and must be serialised by the caller. */
+ * VD_ERR_INVALID_ARG and a message saying how much they need.  Every call
+ * looks up that array's device address with the caller's device current
+ * (the lookup allocates nothing).  With lazy module loading
+ * (CUDA_MODULE_LOADING=LAZY, the default of recent CUDA releases) the first
+ * call on a device may be the one that loads the library's device code and
+ * with it the 8 MiB array, so make that first call before any stream
+ * capture.  Work runs on the legacy default stream; every call reuses the
+ * same scratch, so calls that overlap on one device race and must be
+ * serialised by the caller. */
 vd_status vd_poisson_solve_noalloc(int dim, const int* n_cell, const double* dx,
                                    const int* bc_lo, const int* bc_hi,
                                    const double* bcval_lo, const double* bcval_hi,

@@ -40,3 +40,26 @@ def test_compare_plotfiles(tmp_path):
     assert pf.compare_plotfiles(str(tmp_path / "a"), str(tmp_path / "b"), "A") == (0.0, 0.0)
     err, rel = pf.compare_plotfiles(str(tmp_path / "a"), str(tmp_path / "b"), "B")
     assert 5e-7 < rel < 2e-6
+
+
+def test_reader_takes_per_direction_ghost_widths(tmp_path):
+    """AMReX writes the VisMF ngrow line as an IntVect such as (2,1,0) when
+    the ghost widths differ by direction; the FAB on disk then holds the
+    grown box, and the reader drops each direction's own width."""
+    rng = np.random.default_rng(1)
+    S = rng.uniform(size=(2, 3, 4, 5))          # (ncomp, nz, ny, nx)
+    p = str(tmp_path / "plt")
+    pf.write_plotfile(p, S, ["A", "B"], [0, 0, 0], [1, 1, 1])
+    g = (2, 1, 0)
+    grown = np.full((2, 3 + 2 * g[2], 4 + 2 * g[1], 5 + 2 * g[0]), -7.0)
+    grown[:, g[2]:g[2] + 3, g[1]:g[1] + 4, g[0]:g[0] + 5] = S
+    lvl = os.path.join(p, "Level_0")
+    box = f"(({-g[0]},{-g[1]},{-g[2]}) ({4 + g[0]},{3 + g[1]},{2 + g[2]}) (0,0,0))"
+    with open(os.path.join(lvl, "Cell_D_00000"), "wb") as f:
+        f.write(f"FAB (8, (64 11 52 0 1 12 0 1023))(8, (1 2 3 4 5 6 7 8)){box} 2\n".encode())
+        f.write(np.ascontiguousarray(grown, dtype="<f8").tobytes())
+    hdr = open(os.path.join(lvl, "Cell_H")).read().splitlines()
+    hdr[3] = "(2,1,0)"
+    open(os.path.join(lvl, "Cell_H"), "w").write("\n".join(hdr) + "\n")
+    r = pf.read_plotfile(p)
+    assert np.array_equal(r["data"], S)

@@ -2295,13 +2295,8 @@ namespace {
 
 constexpr long long VD_NA_SCRATCH_DOUBLES = 1LL << 20; // 8 MiB per device
 constexpr int VD_NA_MAX_LEVELS = 16;
-constexpr int VD_NA_MAX_DEVICES = 64;
 
 static __device__ __align__(256) double vd_na_scratch[VD_NA_SCRATCH_DOUBLES];
-
-// Device address of vd_na_scratch per device, looked up once per device
-// with that device current (the host-side symbol is not a device address).
-double* g_na_ptr[VD_NA_MAX_DEVICES] = {};
 
 void na_msg(char* err, int errlen, const char* m)
 {
@@ -2412,13 +2407,18 @@ extern "C" vd_status vd_poisson_solve_noalloc(int dim, const int* n_cell, const 
         na_msg(err, errlen, "vd_poisson_solve_noalloc: bad arguments");
         return VD_ERR_INVALID_ARG;
     }
+    // The host-side name vd_na_scratch is not a device address.  Its device
+    // address is looked up on every call, with the caller's device current:
+    // the lookup allocates nothing, and it stays right after a device reset
+    // or a rebuilt primary context (which reload the module and may move the
+    // array), where an address cached from an earlier call would dangle.
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= VD_NA_MAX_DEVICES)
+    if (cudaGetDevice(&dev) != cudaSuccess)
     {
         na_msg(err, errlen, "vd_poisson_solve_noalloc: no usable current CUDA device");
         return VD_ERR_CUDA;
     }
-    if (!g_na_ptr[dev])
+    double* base = nullptr;
     {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, vd_na_scratch);
@@ -2427,9 +2427,8 @@ extern "C" vd_status vd_poisson_solve_noalloc(int dim, const int* n_cell, const 
             na_msg(err, errlen, cudaGetErrorString(e));
             return VD_ERR_CUDA;
         }
-        g_na_ptr[dev] = static_cast<double*>(p);
+        base = static_cast<double*>(p);
     }
-    double* base = g_na_ptr[dev];
 
     // level hierarchy (fine level: the caller's arrays, natural layout)
     NAHier H{};

@@ -88,7 +88,15 @@ def _read_vismf(level_dir: str, prefix: str, dim: int, dom_lo, dom_hi) -> np.nda
     and offset and placed at its box (ghost cells dropped)."""
     with open(os.path.join(level_dir, f"{prefix}_H")) as f:
         lines = f.read().splitlines()
-    ncomp, ngrow = int(lines[2]), int(lines[3])
+    ncomp = int(lines[2])
+    # ngrow: one width for every direction, or an IntVect "(gx,gy,gz)" when
+    # the widths differ by direction
+    gtxt = lines[3].strip()
+    if gtxt.startswith("("):
+        gw = [int(v) for v in gtxt.strip("()").replace(" ", "").split(",") if v]
+    else:
+        gw = [int(gtxt)] * 3
+    gw = (gw + [0, 0, 0])[:3]
     fabs = [ln.split()[1:] for ln in lines if ln.startswith("FabOnDisk:")]
     n = [dom_hi[d] - dom_lo[d] + 1 for d in range(dim)] + [1] * (3 - dim)
     out = np.zeros((ncomp, n[2], n[1], n[0]))
@@ -102,8 +110,8 @@ def _read_vismf(level_dir: str, prefix: str, dim: int, dom_lo, dom_hi) -> np.nda
             m = [hi[d] - lo[d] + 1 for d in range(dim)] + [1] * (3 - dim)
             raw = f.read(8 * nc * m[0] * m[1] * m[2])
         a = np.frombuffer(raw, dtype=">f8" if big else "<f8").reshape(nc, m[2], m[1], m[0])
-        vlo = [lo[d] + ngrow - dom_lo[d] for d in range(dim)] + [0] * (3 - dim)
-        g = [ngrow] * dim + [0] * (3 - dim)
+        g = [gw[d] for d in range(dim)] + [0] * (3 - dim)
+        vlo = [lo[d] + g[d] - dom_lo[d] for d in range(dim)] + [0] * (3 - dim)
         v = a[:, g[2]:m[2] - g[2], g[1]:m[1] - g[1], g[0]:m[0] - g[0]]
         out[:, vlo[2]:vlo[2] + v.shape[1], vlo[1]:vlo[1] + v.shape[2],
             vlo[0]:vlo[0] + v.shape[3]] = v
