@@ -43,7 +43,8 @@ def _stale(case: str) -> bool:
     if not os.path.exists(out):
         return True
     t = os.path.getmtime(out)
-    deps = [os.path.join(HERE, "vd_oracle.cpp"), os.path.join(ROOT, "include", "vidyut_b200.h")]
+    deps = [os.path.join(HERE, "vd_oracle.cpp"), os.path.join(HERE, "oracle_defaults.H"),
+            os.path.join(ROOT, "include", "vidyut_b200.h")]
     deps += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".H")]
     deps += [os.path.join(CASES, case, f) for f in os.listdir(os.path.join(CASES, case))]
     return any(os.path.getmtime(p) > t for p in deps)
@@ -55,7 +56,8 @@ def build_case(case: str, force: bool = False) -> str:
     if not force and not _stale(case):
         return out
     cmd = [CXX, "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
-           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-I", os.path.join(CASES, case),
+           "-I", HERE, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+           "-I", os.path.join(CASES, case),
            os.path.join(HERE, "vd_oracle.cpp"), "-o", out + ".tmp"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

@@ -40,7 +40,7 @@
 
 #include "vd_vars.H"
 #include "vd_parmparse.H"
-#include "PlasmaChem.H"
+#include "oracle_defaults.H"
 #include <UserFunctions.H>
 #include <UserSources.H>
 #include <Prob.H>
