@@ -7,14 +7,29 @@ verification cases state analytic solutions:
     relative error of 1e-3 (test/verification/MMS2/l2err/l2err.cpp:176-194);
   * Advect (test/verification/Advect/get_error_1d.py): the WENO5 solution
     of sin(pi x - sin(pi x)/pi) advected at unit speed, whose convergence
-    order the case exists to show.
+    order the case exists to show;
+  * MMS2 (test/verification/MMS2): the whole model with the electron-energy
+    equation, Dirichlet species walls and the ionization mechanism, steady
+    n_e = x^3/alpha + n0 and phi = (x^5 - x)/40 within the reference's
+    l2err bound of 1e-3 (l2err/l2err.cpp:176-194), converging at second
+    order;
+  * MMS3 (test/verification/MMS3): time accuracy of the corrector loop,
+    exponential decay of n_e (rate 5) and of the electron energy (rate 10)
+    per cell; one corrector is first order and two are second order
+    (README.md, run1.sh/run2.sh's dt sweep to t = 0.1).
+
+Laplace_2D and Laplace_2D_RobinBC_Test solve on an annulus cut out of the
+box by the immersed-boundary path (vidyut.using_ib = 1), which is outside
+the single-level species-and-field update built here, so they are not
+restated.
 """
 import numpy as np
 import pytest
 
 from oracle.oracle import Oracle
 from tests.cases import (ADVECT_PROB, advect_config, advect_error, mms1_config,
-                         mms1_errors)
+                         mms1_errors, mms2_config, mms2_errors, mms3_config,
+                         mms3_errors)
 
 
 def run_mms1(n, hyp):
@@ -51,3 +66,47 @@ def test_advect_weno_convergence_order(weno, order):
     e = [run_advect(n, weno) for n in (20, 40, 80)]
     assert e[2] < 1e-5
     assert np.log2(e[1] / e[2]) > order, e
+
+
+def run_mms2(n, steps=100):
+    o = Oracle(mms2_config(n))
+    o.init_domain("prob.axial_dir = 0")
+    o.step(steps)
+    S = o.get_state()
+    return mms2_errors(S, n), S
+
+
+def test_mms2_steady_state_within_reference_bound():
+    (ee, ep), S = run_mms2(64)
+    assert ee < 1e-3 and ep < 1e-3, (ee, ep)
+    # the electron energy follows the same cubic profile as the electrons
+    x = (np.arange(64) + 0.5) / 64
+    from tests.cases import MMS2_ALPHA, MMS2_N0
+    from vidyut_b200 import case_info
+    een = S[case_info("mms2")["een_id"]]
+    ex = x ** 3 / MMS2_ALPHA + MMS2_N0
+    assert np.sqrt(np.mean((een - ex) ** 2)) / np.mean(een) < 1e-3
+
+
+def test_mms2_second_order_convergence():
+    (e32, p32), _ = run_mms2(32)
+    (e64, p64), _ = run_mms2(64)
+    assert np.log2(e32 / e64) > 1.8 and np.log2(p32 / p64) > 1.8, (e32, e64, p32, p64)
+
+
+def run_mms3(dt, corr):
+    o = Oracle(mms3_config(dt, corr))
+    o.init_domain("prob.axial_dir = 0")
+    st = o.step(int(round(0.1 / dt)))
+    assert abs(st.time - 0.1) < 1e-12
+    return mms3_errors(o.get_state(), 16, 0.1)
+
+
+@pytest.mark.parametrize("corr,order", [(1, 0.95), (2, 1.95)])
+def test_mms3_time_order(corr, order):
+    e = [run_mms3(dt, corr) for dt in (0.01, 0.005, 0.0025)]
+    for a, b in zip(e, e[1:]):
+        assert np.log2(a[0] / b[0]) > order and np.log2(a[1] / b[1]) > order, e
+    if corr == 2:
+        # the reference's bound at its finest step of the sweep
+        assert run_mms3(0.00125, 2)[0] < 1e-3

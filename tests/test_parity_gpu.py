@@ -207,3 +207,43 @@ def test_lmea_step_parity_energy_equation(require_gpu):
             r = rel(Sg[c], So[c])
             assert r < 1e-11, (s, c, r)
         assert Sg[:8].min() >= cfg["min_species_density"]
+
+
+def test_mms2_known_answer_on_gpu(require_gpu):
+    """The whole model with the electron-energy equation and Dirichlet
+    species walls (test/verification/MMS2) on the GPU: the reference's
+    bound against the analytic steady state, and the oracle's fields."""
+    from tests.cases import mms2_config, mms2_errors
+
+    cfg = mms2_config(64)
+    for k, v in TIGHT.items():
+        cfg[k] = v
+    g, o = pair(cfg, prob="prob.axial_dir = 0")
+    g.step(100)
+    o.step(100)
+    Sg, So = g.get_state(), o.get_state()
+    ee, ep = mms2_errors(Sg, 64)
+    assert ee < 1e-3 and ep < 1e-3, (ee, ep)
+    for c in (0, 2, g.info["een_id"], g.info["etemp_id"], g.info["pot_id"]):
+        assert rel(Sg[c], So[c]) < 1e-10, (c, rel(Sg[c], So[c]))
+
+
+@pytest.mark.parametrize("corr", [1, 2])
+def test_mms3_time_accuracy_on_gpu(require_gpu, corr):
+    """Per-cell decay with one and two correctors (test/verification/MMS3)
+    on the GPU: the orders of the oracle and the oracle's values."""
+    from tests.cases import mms3_config, mms3_errors
+
+    errs = []
+    for dt in (0.01, 0.005):
+        cfg = mms3_config(dt, corr)
+        g, o = pair(cfg, prob="prob.axial_dir = 0")
+        n = int(round(0.1 / dt))
+        g.step(n)
+        o.step(n)
+        Sg, So = g.get_state(), o.get_state()
+        for c in (0, 2, g.info["een_id"]):
+            assert rel(Sg[c], So[c]) < 1e-12, (dt, c, rel(Sg[c], So[c]))
+        errs.append(mms3_errors(Sg, 16, 0.1))
+    order = np.log2(errs[0][0] / errs[1][0])
+    assert order > (0.95 if corr == 1 else 1.95), errs

@@ -1,0 +1,9 @@
+#pragma once
+#include "vd_defs.H"
+
+struct ProbParm
+{
+    int axdir = 0;
+    vd::Real solnfrac = 0.5;
+    vd::Real n0 = 1e6;
+};
