@@ -717,17 +717,27 @@ struct OMG
         }
     }
 
-    // Solve L(sol) = rhs; returns iterations, -1 when maxiter is hit.
+    // Solve L(sol) = rhs; returns iterations, -1 when maxiter is hit.  With
+    // `zero_target` the stopping target is that of a solve from a zero
+    // initial guess, whatever `sol` starts from (a warm-started potential).
     int solve(std::vector<Real>& sol, std::vector<Real> rhs, Real tol_rel,
-              Real tol_abs, vd_solve_stats* st)
+              Real tol_abs, vd_solve_stats* st, bool zero_target = false)
     {
         apply_inhomog_neumann(rhs);
         OLevel& f = L[0];
+        Real rref = -1.0;
+        if (zero_target)
+        {
+            std::vector<Real> z(sol.size(), 0.0);
+            residual(0, z, rhs, f.res, true);
+            rref = norminf(f.res);
+        }
         residual(0, sol, rhs, f.res, true);
         const Real r0 = norminf(f.res);
         // relative to the larger of |rhs| and |r0| (MLMG's "bnorm"/"resid0")
         const Real b0 = norminf(rhs);
-        const Real target = std::max(tol_abs, std::max(tol_rel, 1e-16) * std::max(b0, r0));
+        const Real target =
+            std::max(tol_abs, std::max(tol_rel, 1e-16) * std::max(b0, rref >= 0.0 ? rref : r0));
         if (st)
         {
             st->initial_residual = r0;
@@ -1029,7 +1039,8 @@ void solve_potential(OCtx& c, Real time, Fab& Sborder, Fab& Sborder_old,
             for (int j = 0; j < geo.n[1]; ++j)
                 for (int i = 0; i < geo.n[0]; ++i)
                     sol[OMG::idx(geo, i, j, k)] = sb(i, j, k, POT_ID) / ps;
-    const int it = mg.solve(sol, rhs, cfg.linsolve_reltol, cfg.linsolve_abstol, st);
+    const int it = mg.solve(sol, rhs, cfg.linsolve_reltol, cfg.linsolve_abstol, st,
+                            cfg.poisson_warm_start != 0);
     if (it > 0) c.n_poisson_iters += it;
     if (it < 0) c.n_poisson_iters += cfg.linsolve_maxiter;
 

@@ -208,12 +208,14 @@ def test_adjoint_c4_vs_fd(require_gpu):
       ulp(J) / (2h), about 1.9 at J = 2.3e10 (gradient entries are <= ~900):
       |g - fd| <= 1e-6 |fd| + ulp(J) / h.
     * Central differences formed cell by cell (cell_difference_fd) at
-      h = 1e-4 and h/2, whose truncation error (h^2/6 times the third
-      derivative, ~2e-9 relative for the exponential pre-factor dependence)
-      is negligible; their distance measures the remaining noise.  Bound:
-      |g - D(h/2)| <= 1e-6 |D(h/2)| + 2 |D(h) - D(h/2)|, and on the four
-      large entries that measured noise floor must itself be below 1e-6 of
-      the entry, so that the check resolves 1e-6 relative."""
+      h = 4e-3, 2e-3 and 1e-3, Richardson-extrapolated in pairs,
+      R1 = (4 D(2e-3) - D(4e-3)) / 3 and R2 = (4 D(1e-3) - D(2e-3)) / 3
+      (truncation O(h^4), ~1e-12 relative here).  The per-cell rounding
+      noise of a difference grows as 1/h (6e-7 relative at h = 1e-4 on
+      this workload), so the larger steps keep it near 1e-7; |R1 - R2|
+      measures what remains.  Bound: |g - R2| <= 1e-6 |R2| + 2 |R1 - R2|,
+      and on the four large entries that measured floor must itself be
+      below 1e-6 of the entry, so that the check resolves 1e-6 relative."""
     cfg = W.adjoint_config(128)
     S = W.adjoint_state(cfg, 0)
     g = vb.Vidyut(cfg)
@@ -234,14 +236,14 @@ def test_adjoint_c4_vs_fd(require_gpu):
         assert abs(gr[k] - fd[k]) <= 1e-6 * abs(fd[k]) + ulp / step, (k, gr[k], fd[k])
     dV = float(np.prod([(cfg["prob_hi"][d] - cfg["prob_lo"][d]) / cfg["n_cell"][d]
                         for d in range(3)]))
-    hc = 1e-4
     for k in ks:
-        d1 = cell_difference_fd(g, p, nsteps, k, hc, dV)
-        d2 = cell_difference_fd(g, p, nsteps, k, hc / 2, dV)
-        noise = 2.0 * abs(d1 - d2)
-        assert abs(gr[k] - d2) <= 1e-6 * abs(d2) + noise, (k, gr[k], d1, d2)
+        d4, d2, d1 = (cell_difference_fd(g, p, nsteps, k, hh, dV) for hh in (4e-3, 2e-3, 1e-3))
+        r1 = (4.0 * d2 - d4) / 3.0
+        r2 = (4.0 * d1 - d2) / 3.0
+        noise = 2.0 * abs(r1 - r2)
+        assert abs(gr[k] - r2) <= 1e-6 * abs(r2) + noise, (k, gr[k], r1, r2)
         if k in order[:4]:
-            assert noise <= 1e-6 * abs(gr[k]), (k, gr[k], d1, d2)
+            assert noise <= 1e-6 * abs(gr[k]), (k, gr[k], r1, r2)
 
 
 @pytest.mark.gpu

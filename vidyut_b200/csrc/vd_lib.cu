@@ -611,6 +611,7 @@ struct Ctx
     double* phi_rhs = nullptr;
     double* spec_rhs = nullptr;
     double* r64 = nullptr;  // FP64 residual of the refinement form
+    double* zero64 = nullptr; // all-zero level-0 array (warm-started potential)
     SideArrays pside[6]{}, sside[6]{};
     Hier<double> HP, HS;
     Hier<float> HP32, HS32;
@@ -832,15 +833,18 @@ void bind_sides32(Ctx& c, Hier<float>& H, SideArrays* sides, const int* bct)
 // Solve L(sol) = rhs on the fine level.  Plain: FP64 V-cycles smoothing the
 // solution.  Refined: FP64 residual, FP32 V-cycles on the normalised
 // correction, FP64 update; both stop on |r|_inf <= max(abs, rel |r0|_inf).
+// `r0_ref` >= 0 replaces the initial residual in the stopping target: a
+// solve started from an earlier solution stops where the same solve started
+// from the reference's initial guess would (its residual norm is r0_ref).
 int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* rhs,
-             vd_solve_stats* stats, int hint = 1, bool allow32 = true)
+             vd_solve_stats* stats, int hint = 1, bool allow32 = true, double r0_ref = -1.0)
 {
     const vd_config& cfg = c.cfg;
     double b0 = 0.0;
     const double r0 = resid_norm(c, H64.op[0], sol, rhs, (double*)nullptr, true, &b0);
     // relative to the larger of |rhs| and |r0| (MLMG's "bnorm"/"resid0")
-    const double target =
-        std::max(cfg.linsolve_abstol, std::max(cfg.linsolve_reltol, 1e-16) * std::max(b0, r0));
+    const double target = std::max(cfg.linsolve_abstol, std::max(cfg.linsolve_reltol, 1e-16) *
+                                                            std::max(b0, r0_ref >= 0.0 ? r0_ref : r0));
     vd_solve_stats st{};
     st.initial_residual = r0;
     st.final_residual = r0;
@@ -1029,9 +1033,17 @@ void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats,
         if (c.pbct[s] == MG_INNEU)
             LAUNCH(k_inneu_adjust, gsz(plane_count(c.g, s % 3)), BS, c.st, c.HP.g[0], s,
                    (const double*)nullptr, -1.0, 1.0, c.G.dx[s % 3], c.pside[s].val, c.phi_rhs);
+    // a warm-started solve keeps the stopping target of the reference's
+    // zero-initial-guess solve (Source/PotentialSolve.cpp:479-488): its
+    // initial residual |f - L(0)| (inhomogeneous boundaries), one norm pass
+    // over an all-zero array
+    double r0_zero = -1.0;
+    if (cfg.poisson_warm_start && c.zero64)
+        r0_zero = resid_norm(c, c.HP.op[0], (const double*)c.zero64, (const double*)c.phi_rhs,
+                             (double*)nullptr, true);
     vd_solve_stats st{};
     const int it = mg_solve(c, c.HP, c.HP32, c.phi_sol, c.phi_rhs, &st, c.hint[VD_NT],
-                            !c.HP.varb);
+                            !c.HP.varb, r0_zero);
     if (st.converged && it > 0) c.hint[VD_NT] = it;
     c.poisson_iters += it;
     c.max_poisson_res = std::max(c.max_poisson_res, st.final_residual);
@@ -1905,6 +1917,11 @@ vd_status vd_create(const vd_config* cfg, void** out)
             hier_build(c->HP32, c->A, g, dx, mcl, false, true);
             hier_build(c->HS32, c->A, g, dx, mcl, true, true);
             c->r64 = c->A.get<double>(N);
+        }
+        if (cfg->poisson_warm_start)
+        {
+            c->zero64 = c->A.get<double>(N);
+            VD_CUDA_OK(cudaMemset(c->zero64, 0, sizeof(double) * (size_t)N));
         }
         for (Hier<double>* h : {&c->HP, &c->HS})
         {
