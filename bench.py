@@ -1,10 +1,12 @@
 """Benchmark: cell-steps/s of the per-timestep species-and-field update.
 
-Workload: the 3-D Townsend discharge on a uniform 256^3 grid (2 cm cube,
-20 kV across z, five seeded Gaussian blobs, WENO5-Z drift, dt = 5e-13 s),
-two transported species plus a background gas, FP64 state.  A "step" is one
-full coarse step (Poisson multigrid solve, field, reactions + drift fluxes,
-implicit diffusion multigrid solve per species, write-back).
+Workload (the headline): the 3-D Townsend discharge on a uniform 256^3 grid
+(2 cm cube, 20 kV across z, five seeded Gaussian blobs, WENO5-Z drift,
+dt = 5e-13 s), two transported species plus a background gas, FP64 state,
+in the plain form (the reference's scheme: FP64 multigrid, zero initial
+guess of the potential).  A "step" is one full coarse step (Poisson
+multigrid solve, field, reactions + drift fluxes, implicit diffusion
+multigrid solve per species, write-back).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vidyut_b200|reference]
 
@@ -12,10 +14,16 @@ One process per GPU (torchrun for N > 1); the path does not shard, so N > 1
 runs N independent replicas ("weak" scaling; barrier and max-over-ranks
 device time).  `--impl reference` times the CPU restatement of the reference
 step (the reference, an AMReX application, cannot be built here) on the host
-cores, rank 0 only, on a 96^3 sample of the same workload per step.
+cores, rank 0 only, on the same 256^3 workload.
 
 Timing: device time of the K steps from CUDA events on the library's stream;
-inputs (3.4 GB of state) exceed the 126 MB L2 between steps.
+inputs (3.4 GB of state) exceed the 126 MB L2 between steps.  Extra legs on
+the same line: the other multigrid forms of the same step (FP64 and FP32
+refinement, zero or warm initial guess) with their Poisson error against an
+FP64 solve converged to 1e-13; the step's own roofline from its algorithmic
+bytes; the 512^3 mixed-precision Poisson + implicit-diffusion workload; the
+192^3 LMEA step with the electron-energy equation; the 2-D 256^2 run of 100
+steps; the 128^3 discrete adjoint.
 """
 from __future__ import annotations
 
@@ -52,6 +60,21 @@ def load_traffic():
         with open(p) as f:
             return json.load(f)
     return None
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def host_threads() -> int:
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
 
 
 class Clocks:
@@ -139,16 +162,19 @@ def barrier(dist):
         dist.barrier()
 
 
-def make(n: int, precision: int, device: int):
+def make(n: int, precision: int, device: int, warm: int = 0, **kw):
     from vidyut_b200 import workloads as W
-    cfg = W.townsend_config(3, n)
+    cfg = W.townsend_config(3, n, **kw)
     cfg["mg_precision"] = precision
+    cfg["poisson_warm_start"] = warm
     cfg["device"] = device
     return cfg
 
 
-def cpu_sample(steps: int, n: int = 128) -> dict:
-    """CPU restatement of the reference step, timed on the host cores."""
+def cpu_sample(n: int = 256, steps: int = 2) -> dict:
+    """CPU restatement of the reference step, timed on the host cores on the
+    headline workload itself (a bounded number of steps), plus the 2-D
+    256^2 run of 100 steps in full."""
     from oracle.oracle import Oracle
     from vidyut_b200 import workloads as W
     cfg = W.townsend_config(3, n)
@@ -157,43 +183,86 @@ def cpu_sample(steps: int, n: int = 128) -> dict:
     t0 = time.perf_counter()
     o.step(steps)
     el = time.perf_counter() - t0
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    o.close()
+    c2 = W.townsend_config(2, 256)
+    o2 = Oracle(c2)
+    o2.set_state(0, W.initial_state(c2, 0))
+    t1 = time.perf_counter()
+    o2.step(100)
+    el2 = time.perf_counter() - t1
+    o2.close()
+    cores = host_threads()
     return {"value": n ** 3 * steps / el, "unit": "cell-steps/s", "cores": cores,
-            "kind": "port", "seconds": el,
-            "sample": f"{steps} step(s) of the same workload on a {n}^3 grid "
-                      f"(oracle/vd_oracle.cpp, g++ -O3 -fopenmp, {cores} threads)"}
+            "cpu": cpu_model(), "kind": "port", "seconds": el,
+            "sample": f"{steps} step(s) of the same workload at {n}^3 from the same initial "
+                      f"state (oracle/vd_oracle.cpp, g++ -O3 -fopenmp, {cores} threads)",
+            "townsend_2d_256": {"value": 256 * 256 * 100 / el2, "unit": "cell-steps/s",
+                                "seconds": el2,
+                                "sample": "2-D 256^2, 100 steps at dt 1e-12 s, in full"}}
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the CPU restatement of the reference step on the
+    host cores, on the headline workload (256^3).  The CPU has no warm-up
+    effects worth 10 s steps, so one untimed step stands for the warm-up."""
     if rank != 0:
         return
-    n = 96
+    n = args.n
     from oracle.oracle import Oracle
     from vidyut_b200 import workloads as W
     cfg = W.townsend_config(3, n)
     o = Oracle(cfg)
     o.set_state(0, W.initial_state(cfg, 0))
-    o.step(args.warmup)
+    o.step(1)
     t0 = time.perf_counter()
     o.step(args.steps)
     el = time.perf_counter() - t0
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    cores = host_threads()
     v = n ** 3 * args.steps / el
     line = {
         "metric": "cell-steps/s", "value": v, "unit": "cell-steps/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "townsend_3d (two-species Townsend discharge, WENO5-Z, "
-                               "dt 5e-13 s)", "grid": [n, n, n], "parallelism": "host threads"},
-        "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port",
-                         "sample": f"each step one step of the workload on a {n}^3 grid "
-                                   "(CPU restatement of the reference step; the reference "
-                                   "itself needs AMReX, absent here)"},
+        "config": {"workload": "townsend_3d: two-species Townsend discharge + background "
+                               "gas, 2 cm cube, 20 kV across z, 5 seeded blobs, WENO5-Z, "
+                               "dt 5e-13 s, FP64 multigrid (reference scheme)",
+                   "grid": [n, n, n], "parallelism": "host threads"},
+        "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores, "cpu": cpu_model(),
+                         "kind": "port",
+                         "sample": f"{args.steps} steps of the workload at {n}^3 after one "
+                                   "untimed step (CPU restatement of the reference step; the "
+                                   "reference itself needs AMReX, absent here)"},
         "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# Algorithmic bytes per cell of the step's kernels: one read of each
+# distinct input array and one write of each output per launch (FP64 8 B,
+# FP32 4 B), the per-kernel table of the path's measurement plan.
+B_POISSON_RHS = 24.0
+B_VCYCLE64 = (4 * 24 + 17 + 17) * 8.0 / 7.0      # constant coefficients, V(2,2)
+B_VCYCLE32 = B_VCYCLE64 / 2.0
+B_VCYCLE64_VAR = (4 * 32 + 17 + 17) * 8.0 / 7.0  # face coefficients (species)
+B_REFINE = 40.0                                  # FP64 residual 20 + update 20
+B_EFIELD = 64.0
+B_EXPLICIT = 72.0
+B_SPECIES_SETUP = 24.0
+B_FINALIZE = 16.0
+
+
+def step_bytes(pv: float, sv: float, nspec: int, refines: float = 0.0,
+               fp32: bool = False, warm: bool = False) -> float:
+    """B_step per cell for the Townsend step: RHS, n_V potential V-cycles,
+    E field, explicit sources, per species set-up + its V-cycles, finalize;
+    the refined form's FP64 refinement passes; a warm start's extra norm
+    pass over the zero-guess residual (16 B)."""
+    b = B_POISSON_RHS + pv * (B_VCYCLE32 if fp32 else B_VCYCLE64) + B_EFIELD + B_EXPLICIT
+    b += nspec * B_SPECIES_SETUP + sv * B_VCYCLE64_VAR + nspec * B_FINALIZE
+    b += refines * B_REFINE + (16.0 if warm else 0.0)
+    return b
 
 
 def timed(g, steps: int, dist, prof_id: int):
@@ -245,6 +314,135 @@ def adjoint_leg(device: int, dist, n: int = 128, nsteps: int = 50, K: int = 10) 
             "objective": J, "grad_norm": float(np.linalg.norm(grad))}
 
 
+def forms_leg(n: int, state, device: int, warmup: int, steps: int, dist, ref_ms: float) -> dict:
+    """The other multigrid forms of the headline step: FP64 or FP32
+    V-cycles (the FP32 ones inside FP64 iterative refinement), potential
+    started from zero (the reference) or from the last potential with the
+    zero-guess stopping target.  Each is timed like the headline (device
+    time of K steps after W warm-up steps) and its Poisson error is measured
+    on one solve from the state after 5 steps of the plain form, against an
+    FP64 solve of the same state converged to 1e-13 (RMS difference over the
+    mean magnitude)."""
+    import vidyut_b200 as vb
+    pid = vb.case_info("townsend")["pot_id"]
+    g = vb.Vidyut(make(n, vb.VD_MG_FP64, device))
+    g.set_state(0, state)
+    g.step(5)
+    s5 = g.get_state()
+    g.close()
+    g = vb.Vidyut(make(n, vb.VD_MG_FP64, device, linsolve_reltol=1e-13, linsolve_abstol=0.0))
+    g.set_state(0, s5)
+    g.solve_potential(0.0)
+    ref = g.get_state(pid, 1)
+    g.close()
+    out = {}
+    for name, prec, warm in (("fp64", vb.VD_MG_FP64, 0), ("fp64_warm", vb.VD_MG_FP64, 1),
+                             ("fp32_refined", vb.VD_MG_FP32_REFINED, 0),
+                             ("fp32_refined_warm", vb.VD_MG_FP32_REFINED, 1)):
+        g = vb.Vidyut(make(n, prec, device, warm))
+        g.set_state(0, s5)
+        sol = g.solve_potential(0.0)
+        phi = g.get_state(pid, 1)
+        err = float(np.sqrt(np.mean((phi - ref) ** 2)) / np.mean(np.abs(ref)))
+        g.set_state(0, state)
+        g.step(warmup)
+        st, _, _ = timed(g, steps, dist, 0)
+        g.close()
+        ms = dist_max(dist, st.gpu_ms) / steps
+        pv, sv = st.poisson_iterations / steps, st.species_iterations / steps
+        refs = st.poisson_refinements / steps
+        out[name] = {"ms_per_step": ms, "speedup_vs_plain_fp64": ref_ms / ms,
+                     "poisson_vcycles_per_step": pv, "species_vcycles_per_step": sv,
+                     "poisson_refinements_per_step": refs,
+                     "poisson_rel_err_vs_fp64_1e-13": err,
+                     "poisson_solve_vcycles_on_error_state": sol.iterations,
+                     "step_bytes_per_cell": step_bytes(pv, sv, 2, refs,
+                                                       prec == vb.VD_MG_FP32_REFINED, warm == 1)}
+    return out
+
+
+def step_roofline(ms_per_step: float, ncell: int, bytes_per_cell: float, peak: float,
+                  peak_kind: str) -> dict:
+    ach = ncell * bytes_per_cell / (ms_per_step / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "peak_kind": peak_kind, "bytes_per_cell": bytes_per_cell,
+            "note": "algorithmic bytes of the whole step (per-kernel table, measured V-cycle "
+                    "counts) over its device time"}
+
+
+def mgsolve_leg(device: int, n: int = 512, reps: int = 3) -> dict:
+    """The 512^3 mixed-precision Poisson + implicit-diffusion workload: the
+    potential solve and the ion's implicit-diffusion solve in the FP64 form
+    and the FP32-refined form (FP32 V(2,2) cycles, 7 levels, inside FP64
+    refinement to the reference's 1e-10 relative residual), host-timed
+    around each synchronous solve (tens of ms each), best of `reps` after
+    one warm-up; error of each form against the FP64 form at 1e-13."""
+    import torch
+    import vidyut_b200 as vb
+    from vidyut_b200 import workloads as W
+    pid = vb.case_info("mgsolve")["pot_id"]
+    expl = np.zeros((3, n, n, n))
+    res = {}
+    ref = {}
+    for name, kw in (("tight", dict(linsolve_reltol=1e-13, linsolve_abstol=0.0)),
+                     ("fp64", dict(mg_precision=vb.VD_MG_FP64)),
+                     ("fp32_refined", dict(mg_precision=vb.VD_MG_FP32_REFINED))):
+        cfg = W.mgsolve_config(n, device=device, **kw)
+        g = vb.Vidyut(cfg)
+        W.mgsolve_load(g, cfg, 0)
+        times_p, times_d = [], []
+        for r in range(reps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sp = g.solve_potential(0.0)
+            t1 = time.perf_counter()
+            if r == 0:
+                phi = g.get_state(pid, 1)
+                ion0 = g.get_state(1, 1)
+            g.set_state(1, ion0)
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            sd = g.implicit_solve_scalar(1, expl, 0.0)
+            t3 = time.perf_counter()
+            if r == 0:
+                ion = g.get_state(1, 1)
+            g.set_state(1, ion0)
+            if r > 0:
+                times_p.append(t1 - t0)
+                times_d.append(t3 - t2)
+        g.close()
+        if name == "tight":
+            ref = {"phi": phi, "ion": ion}
+            continue
+        ep = float(np.sqrt(np.mean((phi - ref["phi"]) ** 2)) / np.mean(np.abs(ref["phi"])))
+        ed = float(np.sqrt(np.mean((ion - ref["ion"]) ** 2)) / np.mean(np.abs(ref["ion"])))
+        res[name] = {"poisson_ms": 1e3 * min(times_p), "poisson_vcycles": sp.iterations,
+                     "poisson_refinements": sp.refinements, "poisson_rel_err": ep,
+                     "diffusion_ms": 1e3 * min(times_d), "diffusion_vcycles": sd.iterations,
+                     "diffusion_rel_err": ed,
+                     "poisson_bytes_per_cell": sp.iterations * (B_VCYCLE32 if name != "fp64"
+                                                                else B_VCYCLE64)
+                     + sp.refinements * B_REFINE}
+    res["poisson_speedup_fp32_refined"] = res["fp64"]["poisson_ms"] / res["fp32_refined"]["poisson_ms"]
+    res["workload"] = (f"{n}^3 unit cube, 8 seeded +-1e16 m^-3 Gaussians of net charge + 1e-3 "
+                       "white noise, Dirichlet z / Neumann x-y; ion diffusivity log-uniform "
+                       "1e-6-1e-1 m^2/s cell by cell, dt 1e-11 s; rel tol 1e-10")
+    return res
+
+
+def steps_leg(cfg, state, warmup: int, steps: int) -> dict:
+    import vidyut_b200 as vb
+    g = vb.Vidyut(cfg)
+    g.set_state(0, state)
+    g.step(warmup)
+    st = g.step(steps)
+    g.close()
+    nc = int(np.prod([cfg["n_cell"][d] for d in range(cfg["dim"])]))
+    return {"ms_per_step": st.gpu_ms / steps, "cell_steps_per_s": nc * steps / (st.gpu_ms / 1e3),
+            "poisson_vcycles_per_step": st.poisson_iterations / steps,
+            "species_vcycles_per_step": st.species_iterations / steps, "steps": steps}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -254,6 +452,9 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the other multigrid forms")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the 512^3 solver, 192^3 LMEA and 2-D legs")
     ap.add_argument("--lean", action="store_true",
                     help="timed FP64 leg only (no e2e, FP32 or CPU legs): profiling runs")
     args = ap.parse_args()
@@ -304,7 +505,8 @@ def main():
             "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
             "algorithmic_bytes_per_launch": pbytes, "launches_timed": nl,
             "avg_launch_us": avg_s * 1e6 if nl else None,
-            "pass": f"second run of the {args.steps} timed steps with per-launch events "
+            "pass": f"second run of the {args.steps} timed steps with per-launch events, "
+                    "V-cycles one at a time so that every timed sweep does its work "
                     f"({ms_p / args.steps:.3f} ms/step under the events)",
             "traffic": (traffic or {}).get("bytes_per_launch") if traffic else None,
             "traffic_note": (traffic or {}).get("note") if traffic else None}
@@ -345,32 +547,29 @@ def main():
                    "wall clock"}
     g.close()
 
-    # FP32-refined multigrid form on the same workload
-    cfg32 = make(n, vb.VD_MG_FP32_REFINED, local)
-    g32 = vb.Vidyut(cfg32)
-    g32.set_state(0, state)
-    g32.step(args.warmup)
-    st32, _, _ = timed(g32, args.steps, dist, 0)
-    ms32 = dist_max(dist, st32.gpu_ms)
-    value32 = replica_value(world, ncell, args.steps, ms32)
-    # Poisson error of the refined form against the FP64 form, same state
-    ga, gb = vb.Vidyut(make(n, vb.VD_MG_FP64, local)), g32
-    ga.set_state(0, state)
-    gb.set_state(0, state)
-    ga.solve_potential(0.0)
-    gb.solve_potential(0.0)
-    pa = ga.get_state(info["pot_id"], 1)
-    pb = gb.get_state(info["pot_id"], 1)
-    perr = float(np.linalg.norm(pb - pa) / np.linalg.norm(pa))
-    ga.close()
-    gb.close()
+    # the other multigrid forms of the same step
+    forms = None if args.no_forms else forms_leg(n, state, local, args.warmup, args.steps, dist,
+                                                 ms / args.steps)
+    solver_legs = {}
+    if not args.no_extra:
+        from vidyut_b200 import workloads as W
+        solver_legs["mgsolve_512"] = mgsolve_leg(local)
+        c2 = W.lmea_config(192, device=local)
+        solver_legs["lmea_192"] = steps_leg(c2, W.lmea_state(c2, 0), 2, 5)
+        solver_legs["lmea_192"]["workload"] = (
+            "LMEA 8 species / 30 reactions + electron-energy equation, 192^3, dt 1e-12 s, "
+            "FP64 plain form")
+        c0 = W.townsend_config(2, 256, device=local)
+        solver_legs["townsend_2d_256"] = steps_leg(c0, W.initial_state(c0, 0), 3, 100)
+        solver_legs["townsend_2d_256"]["workload"] = "2-D 256^2 Townsend, 100 steps at dt 1e-12 s"
 
     adj = None if args.no_adjoint else adjoint_leg(local, dist)
 
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
-            cpu = cpu_sample(8, 128)
+            cpu = cpu_sample(n, 2)
+        pv, sv = st.poisson_iterations / args.steps, st.species_iterations / args.steps
         line = {
             "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -385,15 +584,19 @@ def main():
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": roof,
+            "step_roofline": step_roofline(ms / args.steps, ncell, step_bytes(pv, sv, 2),
+                                           peak, peak_kind),
             "cpu_baseline": cpu,
-            "solver": {"poisson_vcycles_per_step": st.poisson_iterations / args.steps,
-                       "species_vcycles_per_step": st.species_iterations / args.steps},
-            "fp32_refined": {"value": value32, "ms_per_step": ms32 / args.steps,
-                             "speedup_vs_fp64": value32 / value,
-                             "poisson_rel_err_vs_fp64": perr,
-                             "poisson_vcycles_per_step": st32.poisson_iterations / args.steps},
+            "solver": {"poisson_vcycles_per_step": pv, "species_vcycles_per_step": sv},
+            "forms": forms,
+            "solver_workloads": solver_legs or None,
             "adjoint": adj,
         }
+        if forms:
+            for k, f in forms.items():
+                f["step_roofline_frac"] = step_roofline(f["ms_per_step"], ncell,
+                                                        f["step_bytes_per_cell"], peak,
+                                                        peak_kind)["frac"]
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -181,6 +181,8 @@ typedef struct vd_step_stats {
     double dt_edrift;        /* electron time scales of the last step's    */
     double dt_ediff;         /* starting state (adaptive_dt only; DBL_MAX  */
     double dt_diel_relax;    /* where undefined): Source/TimeStep.cpp:46-134 */
+    int poisson_refinements; /* FP64 refinement passes of the potential
+                                solves (FP32-refined form), summed        */
 } vd_step_stats;
 
 /* Kernels that vd_profile_kernel can time launch by launch. */

@@ -1,0 +1,87 @@
+"""Mixed-precision Poisson and implicit diffusion on the solver workload
+(unit cube, 8 seeded +-1e16 m^-3 Gaussians of net charge plus 1e-3 white
+noise, Dirichlet z / Neumann x-y, ion diffusivity log-uniform 1e-6-1e-1
+m^2/s cell by cell, dt = 1e-11 s; vidyut_b200/workloads.py mgsolve_*).
+
+* At 96^3 both precision forms against the CPU oracle converged to 1e-13:
+  the FP64 form at 1e-13 agrees to 1e-11; the FP32-refined form at the
+  reference tolerance (rel 1e-10) is within 1e-10 (the precision target).
+* At 512^3 (the workload's size, 7 multigrid levels) the FP32-refined
+  potential and diffusion solution against the library's FP64 form
+  converged to 1e-13 (the GPU FP64 solver is the oracle's twin at 256^3,
+  tests/test_fullsize_gpu.py): within 1e-10.
+"""
+import numpy as np
+import pytest
+
+import vidyut_b200 as vb
+from oracle.oracle import Oracle
+from vidyut_b200 import workloads as W
+from vidyut_b200.compare import field_error
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = dict(linsolve_reltol=1e-13, linsolve_abstol=0.0)
+
+
+def rel(a, b):
+    return field_error(b, a)[1]
+
+
+def solve_both(g, S, expl):
+    g.set_state(0, S)
+    sp = g.solve_potential(0.0)
+    phi = g.get_state(g.info["pot_id"], 1)
+    g.set_state(0, S)
+    sd = g.implicit_solve_scalar(1, expl, 0.0)
+    ion = g.get_state(1, 1)
+    return sp, sd, phi, ion
+
+
+def test_mgsolve_parity_96(require_gpu):
+    cfg = W.mgsolve_config(96, **TIGHT)
+    S = W.mgsolve_state(cfg, 1)
+    expl = np.zeros((3,) + S.shape[1:])
+    o = Oracle(cfg)
+    _, _, phi_o, ion_o = solve_both(o, S, expl)
+    o.close()
+    g = vb.Vidyut(cfg)
+    sp, sd, phi_g, ion_g = solve_both(g, S, expl)
+    assert sp.converged and sd.converged
+    assert rel(phi_g, phi_o) < 1e-11 and rel(ion_g, ion_o) < 1e-12
+    g.close()
+    r = vb.Vidyut(W.mgsolve_config(96, mg_precision=vb.VD_MG_FP32_REFINED))
+    sp, sd, phi_r, ion_r = solve_both(r, S, expl)
+    assert sp.converged and sp.refinements >= 1
+    assert rel(phi_r, phi_o) <= 1e-10, rel(phi_r, phi_o)
+    assert rel(ion_r, ion_o) <= 1e-10
+
+
+def test_mgsolve_512_refined_error(require_gpu):
+    n = 512
+    cfg = W.mgsolve_config(n)
+    pid = vb.case_info("mgsolve")["pot_id"]
+    expl = None
+
+    def solve(c):
+        nonlocal expl
+        g = vb.Vidyut(c)
+        W.mgsolve_load(g, c, 0)
+        if expl is None:
+            expl = np.zeros((3, n, n, n))
+        sp = g.solve_potential(0.0)
+        phi = g.get_state(pid, 1)
+        sd = g.implicit_solve_scalar(1, expl, 0.0)
+        ion = g.get_state(1, 1)
+        g.close()
+        assert sp.converged and sd.converged
+        return sp, phi, ion
+
+    _, phi_t, ion_t = solve(W.mgsolve_config(n, **TIGHT))
+    errs = {}
+    for prec in (vb.VD_MG_FP64, vb.VD_MG_FP32_REFINED):
+        sp, phi, ion = solve(W.mgsolve_config(n, mg_precision=prec))
+        errs[prec] = (rel(phi, phi_t), rel(ion, ion_t), sp.iterations, sp.refinements)
+    assert errs[vb.VD_MG_FP32_REFINED][0] <= 1e-10, errs
+    assert errs[vb.VD_MG_FP32_REFINED][1] <= 1e-10, errs
+    assert errs[vb.VD_MG_FP32_REFINED][3] >= 1, errs

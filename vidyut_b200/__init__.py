@@ -92,7 +92,8 @@ class vd_step_stats(C.Structure):
                 ("species_iterations", C.c_int), ("not_converged", C.c_int),
                 ("max_poisson_final_residual", C.c_double), ("time", C.c_double),
                 ("gpu_ms", C.c_double), ("dt", C.c_double), ("dt_edrift", C.c_double),
-                ("dt_ediff", C.c_double), ("dt_diel_relax", C.c_double)]
+                ("dt_ediff", C.c_double), ("dt_diel_relax", C.c_double),
+                ("poisson_refinements", C.c_int)]
 
 
 EXPORTS = [

@@ -1,6 +1,6 @@
 """Run the benchmark workload for an external profiler (ncu and the like).
 
-    python -m vidyut_b200.runstep [--n 256] [--warmup 3] [--steps 1] [--fp32]
+    python -m vidyut_b200.runstep [--n 256] [--warmup 3] [--steps 1] [--fp32] [--warm]
     python -m vidyut_b200.runstep --n 208 --solve           # one field solve
     python -m vidyut_b200.runstep --n 192 --solve --explicit  # + explicit sources
 
@@ -26,6 +26,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--fp32", action="store_true", help="FP32-refined multigrid form")
+    ap.add_argument("--warm", action="store_true",
+                    help="start each potential solve from the last potential")
+    ap.add_argument("--inner", type=int, default=0, help="FP32 V-cycles per refinement pass")
     ap.add_argument("--solve", action="store_true", help="one field solve instead of steps")
     ap.add_argument("--explicit", action="store_true", help="with --solve: explicit sources too")
     a = ap.parse_args()
@@ -36,6 +39,10 @@ def main() -> None:
     cfg = W.townsend_config(3, a.n)
     if a.fp32:
         cfg["mg_precision"] = vb.VD_MG_FP32_REFINED
+    if a.warm:
+        cfg["poisson_warm_start"] = 1
+    if a.inner > 0:
+        cfg["mg_inner_cycles"] = a.inner
     g = vb.Vidyut(cfg)
     g.set_state(0, W.initial_state(cfg, 0))
     if a.solve:

@@ -198,3 +198,80 @@ def adjoint_state(cfg: Config, seed: int = 0, efield: float = 1e6) -> np.ndarray
     S[info["efx_id"] + 2] = ez
     S[info["etemp_id"]] = TE_1EV * (1.0 + 0.25 * wave())
     return S
+
+
+def mgsolve_config(n: int, **kw) -> Config:
+    """Mixed-precision Poisson and implicit-diffusion workload: unit cube,
+    n^3 cells, 7-point Laplacian, Dirichlet (0 V) on the z faces and
+    homogeneous Neumann on x and y, for the potential and the diffusing
+    ion alike; implicit diffusion at dt = 1e-11 s."""
+    cfg = Config("mgsolve")
+    cfg["dim"] = 3
+    cfg["n_cell"] = [n, n, n]
+    cfg["prob_hi"] = [1.0, 1.0, 1.0]
+    cfg["dt"] = 1e-11
+    cfg["do_reactions"] = 0
+    cfg["bound_specden"] = 0
+    for key in ("pot", "eden", "ion", "neutral", "eenrg"):
+        cfg[f"{key}_bc_lo"] = [2, 2, 1]
+        cfg[f"{key}_bc_hi"] = [2, 2, 1]
+    for k, v in kw.items():
+        cfg[k] = v
+    return cfg
+
+
+def mgsolve_fields(cfg: Config, seed: int = 0):
+    """Electron density, ion density and ion diffusivity of the solver
+    workload, each (nz, ny, nx): net charge n_ion - n_e of eight seeded
+    Gaussians of amplitude +-1e16 m^-3 (random sign, centres uniform in the
+    middle 80 % of the cube, sigma uniform in 0.03-0.1 of the edge) plus
+    white noise of 1e-3 of that amplitude, on a uniform 1e17 m^-3 electron
+    background; diffusivity log-uniform in 1e-6-1e-1 m^2/s cell by cell."""
+    nx, ny, nz = cfg["n_cell"]
+    rng = np.random.default_rng(seed)
+    amp = 1e16
+    c = rng.uniform(0.1, 0.9, size=(8, 3))
+    sg = rng.uniform(0.03, 0.1, size=8)
+    sgn = rng.choice([-1.0, 1.0], size=8)
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    z = (np.arange(nz) + 0.5) / nz
+    rho = np.zeros((nz, ny, nx))
+    for b in range(8):
+        gx = np.exp(-((x - c[b, 0]) ** 2) / (2 * sg[b] ** 2))
+        gy = np.exp(-((y - c[b, 1]) ** 2) / (2 * sg[b] ** 2))
+        gz = np.exp(-((z - c[b, 2]) ** 2) / (2 * sg[b] ** 2))
+        rho += (sgn[b] * amp) * gz[:, None, None] * gy[None, :, None] * gx[None, None, :]
+    rho += 1e-3 * amp * rng.standard_normal(size=rho.shape)
+    ne = np.full((nz, ny, nx), 1e17)
+    nion = rho
+    nion += 1e17
+    D = 10.0 ** rng.uniform(-6.0, -1.0, size=rho.shape)
+    return ne, nion, D
+
+
+def mgsolve_state(cfg: Config, seed: int = 0) -> np.ndarray:
+    """The full state of the solver workload (mgsolve_fields, with the ion
+    diffusivity in the electron-temperature slot, see
+    cases/mgsolve/Chemistry.H)."""
+    info = case_info(cfg.case)
+    ne, nion, D = mgsolve_fields(cfg, seed)
+    S = np.zeros((info["nvar"],) + ne.shape)
+    S[0] = ne
+    S[1] = nion
+    S[info["etemp_id"]] = D
+    S[info["cmask_id"]] = 1.0
+    return S
+
+
+def mgsolve_load(g, cfg: Config, seed: int = 0) -> None:
+    """Copy the solver workload into a context component by component (at
+    512^3 the full state would be 27 GB of host memory; the context starts
+    from an all-zero state)."""
+    info = case_info(cfg.case)
+    ne, nion, D = mgsolve_fields(cfg, seed)
+    g.set_state(0, ne)
+    g.set_state(1, nion)
+    g.set_state(info["etemp_id"], D)
+    D.fill(1.0)
+    g.set_state(info["cmask_id"], D)
