@@ -384,17 +384,20 @@ def mgsolve_leg(device: int, n: int = 512, reps: int = 3) -> dict:
     expl = np.zeros((3, n, n, n))
     res = {}
     ref = {}
-    for name, kw in (("tight", dict(linsolve_reltol=1e-13, linsolve_abstol=0.0)),
+    # the FP64 reference: solved to the rounding floor (rel 1e-14 is out of
+    # FP64's reach for this right-hand side; 60 V-cycles, status ignored)
+    for name, kw in (("tight", dict(linsolve_reltol=1e-14, linsolve_abstol=0.0,
+                                    linsolve_maxiter=60)),
                      ("fp64", dict(mg_precision=vb.VD_MG_FP64)),
                      ("fp32_refined", dict(mg_precision=vb.VD_MG_FP32_REFINED))):
         cfg = W.mgsolve_config(n, device=device, **kw)
         g = vb.Vidyut(cfg)
         W.mgsolve_load(g, cfg, 0)
         times_p, times_d = [], []
-        for r in range(reps + 1):
+        for r in range(1 if name == "tight" else reps + 1):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            sp = g.solve_potential(0.0)
+            sp = g.solve_potential(0.0, allow_unconverged=name == "tight")
             t1 = time.perf_counter()
             if r == 0:
                 phi = g.get_state(pid, 1)
@@ -402,7 +405,7 @@ def mgsolve_leg(device: int, n: int = 512, reps: int = 3) -> dict:
             g.set_state(1, ion0)
             torch.cuda.synchronize()
             t2 = time.perf_counter()
-            sd = g.implicit_solve_scalar(1, expl, 0.0)
+            sd = g.implicit_solve_scalar(1, expl, 0.0, allow_unconverged=name == "tight")
             t3 = time.perf_counter()
             if r == 0:
                 ion = g.get_state(1, 1)
@@ -413,6 +416,7 @@ def mgsolve_leg(device: int, n: int = 512, reps: int = 3) -> dict:
         g.close()
         if name == "tight":
             ref = {"phi": phi, "ion": ion}
+            res["fp64_reference_residual_ratio"] = sp.final_residual / sp.initial_residual
             continue
         ep = float(np.sqrt(np.mean((phi - ref["phi"]) ** 2)) / np.mean(np.abs(ref["phi"])))
         ed = float(np.sqrt(np.mean((ion - ref["ion"]) ** 2)) / np.mean(np.abs(ref["ion"])))

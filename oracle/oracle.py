@@ -104,7 +104,7 @@ class Oracle:
         self.lib.vdo_step(self.ctx, nsteps, C.byref(st))
         return st
 
-    def solve_potential(self, time: float = 0.0) -> "vb.vd_solve_stats":
+    def solve_potential(self, time: float = 0.0, allow_unconverged: bool = True) -> "vb.vd_solve_stats":
         st = vb.vd_solve_stats()
         self.lib.vdo_poisson_solve(self.ctx, time, C.byref(st))
         return st
@@ -115,7 +115,8 @@ class Oracle:
         self.lib.vdo_explicit_rhs(self.ctx, time, _ptr(out))
         return out
 
-    def implicit_solve_scalar(self, specid: int, expl_src: np.ndarray, time: float = 0.0):
+    def implicit_solve_scalar(self, specid: int, expl_src: np.ndarray, time: float = 0.0,
+                              allow_unconverged: bool = True):
         a = np.ascontiguousarray(expl_src, dtype=np.float64)
         st = vb.vd_solve_stats()
         self.lib.vdo_implicit_diffusion(self.ctx, specid, time, _ptr(a), C.byref(st))

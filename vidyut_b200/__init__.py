@@ -334,9 +334,11 @@ class Vidyut:
             self._chk(r, "vd_step")
         return st
 
-    def solve_potential(self, time: float = 0.0) -> vd_solve_stats:
+    def solve_potential(self, time: float = 0.0, allow_unconverged: bool = False) -> vd_solve_stats:
         st = vd_solve_stats()
-        self._chk(self.lib.vd_poisson_solve(self.ctx, time, C.byref(st)), "vd_poisson_solve")
+        r = self.lib.vd_poisson_solve(self.ctx, time, C.byref(st))
+        if not (allow_unconverged and r == 3):
+            self._chk(r, "vd_poisson_solve")
         return st
 
     def explicit_rhs(self, time: float = 0.0) -> np.ndarray:
@@ -346,11 +348,12 @@ class Vidyut:
         return out
 
     def implicit_solve_scalar(self, specid: int, expl_src: np.ndarray,
-                              time: float = 0.0) -> vd_solve_stats:
+                              time: float = 0.0, allow_unconverged: bool = False) -> vd_solve_stats:
         a = np.ascontiguousarray(expl_src, dtype=np.float64)
         st = vd_solve_stats()
-        self._chk(self.lib.vd_implicit_diffusion(self.ctx, specid, time, _ptr(a), 0,
-                                                 C.byref(st)), "vd_implicit_diffusion")
+        r = self.lib.vd_implicit_diffusion(self.ctx, specid, time, _ptr(a), 0, C.byref(st))
+        if not (allow_unconverged and r == 3):
+            self._chk(r, "vd_implicit_diffusion")
         return st
 
     def check_state(self) -> int:
