@@ -381,7 +381,9 @@ def mgsolve_leg(device: int, n: int = 512, reps: int = 3) -> dict:
     import vidyut_b200 as vb
     from vidyut_b200 import workloads as W
     pid = vb.case_info("mgsolve")["pot_id"]
-    expl = np.zeros((3, n, n, n))
+    # explicit sources on the device (zero: pure implicit diffusion), so the
+    # timed diffusion solve holds no host copy
+    expl = torch.zeros((3, n, n, n), dtype=torch.float64, device=f"cuda:{device}")
     res = {}
     ref = {}
     # the FP64 reference: solved to the rounding floor (rel 1e-14 is out of

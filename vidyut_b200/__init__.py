@@ -349,9 +349,15 @@ class Vidyut:
 
     def implicit_solve_scalar(self, specid: int, expl_src: np.ndarray,
                               time: float = 0.0, allow_unconverged: bool = False) -> vd_solve_stats:
-        a = np.ascontiguousarray(expl_src, dtype=np.float64)
         st = vd_solve_stats()
-        r = self.lib.vd_implicit_diffusion(self.ctx, specid, time, _ptr(a), 0, C.byref(st))
+        if getattr(expl_src, "is_cuda", False):
+            # a contiguous FP64 CUDA tensor on the context's device: no copy
+            assert expl_src.is_contiguous() and str(expl_src.dtype) == "torch.float64"
+            r = self.lib.vd_implicit_diffusion(self.ctx, specid, time,
+                                               C.c_void_p(expl_src.data_ptr()), 1, C.byref(st))
+        else:
+            a = np.ascontiguousarray(expl_src, dtype=np.float64)
+            r = self.lib.vd_implicit_diffusion(self.ctx, specid, time, _ptr(a), 0, C.byref(st))
         if not (allow_unconverged and r == 3):
             self._chk(r, "vd_implicit_diffusion")
         return st

@@ -31,11 +31,32 @@ def main() -> None:
     ap.add_argument("--inner", type=int, default=0, help="FP32 V-cycles per refinement pass")
     ap.add_argument("--solve", action="store_true", help="one field solve instead of steps")
     ap.add_argument("--explicit", action="store_true", help="with --solve: explicit sources too")
+    ap.add_argument("--mgsolve", action="store_true",
+                    help="the solver workload (workloads.mgsolve_*): one warm-up and one "
+                         "timed potential solve")
     a = ap.parse_args()
 
     import vidyut_b200 as vb
     from vidyut_b200 import workloads as W
 
+    if a.mgsolve:
+        import time
+        cfg = W.mgsolve_config(a.n)
+        if a.fp32:
+            cfg["mg_precision"] = vb.VD_MG_FP32_REFINED
+        if a.inner > 0:
+            cfg["mg_inner_cycles"] = a.inner
+        g = vb.Vidyut(cfg)
+        W.mgsolve_load(g, cfg, 0)
+        g.solve_potential(0.0)
+        l0 = g.launch_count()
+        t0 = time.perf_counter()
+        st = g.solve_potential(0.0)
+        el = time.perf_counter() - t0
+        print(f"timed solve: {g.launch_count() - l0} launches, {1e3 * el:.3f} ms, "
+              f"V-cycles {st.iterations}, refinements {st.refinements}")
+        g.close()
+        return
     cfg = W.townsend_config(3, a.n)
     if a.fp32:
         cfg["mg_precision"] = vb.VD_MG_FP32_REFINED
