@@ -65,10 +65,38 @@ def build_case(case: str, force: bool = False, extra: list[str] | None = None) -
     return out
 
 
+HOST = os.path.join(PKG, "host", "vd_run.cpp")
+
+
+def host_path(case: str) -> str:
+    return os.path.join(LIBDIR, f"vd_run_{case}")
+
+
+def build_host(case: str, force: bool = False) -> str:
+    """The C++ host driver (host/vd_run.cpp) linked against one case
+    library through the C ABI only (include/vidyut_b200.h)."""
+    lib = build_case(case)
+    out = host_path(case)
+    if (not force and os.path.exists(out) and
+            os.path.getmtime(out) >= max(os.path.getmtime(HOST), os.path.getmtime(lib))):
+        return out
+    cxx = os.environ.get("CXX", "g++")
+    cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), HOST,
+           "-L", LIBDIR, f"-lvd_{case}", "-Wl,-rpath,$ORIGIN", "-o", out + ".tmp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host build failed for case {case}:\n{r.stderr[-4000:]}")
+    os.replace(out + ".tmp", out)
+    return out
+
+
 def build_all(force: bool = False) -> list[str]:
     cs = cases()
     with ThreadPoolExecutor(max_workers=min(4, len(cs))) as ex:
-        return list(ex.map(lambda c: build_case(c, force), cs))
+        out = list(ex.map(lambda c: build_case(c, force), cs))
+    for c in cs:
+        build_host(c, force)
+    return out
 
 
 if __name__ == "__main__":
