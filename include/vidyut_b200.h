@@ -148,6 +148,17 @@ typedef struct vd_config {
                                 potential (reference: zero guess,
                                 Source/PotentialSolve.cpp:479-485)       */
     int device;              /* CUDA device ordinal                        */
+
+    /* multicomponent species solves (Source/Evolve.cpp:458-573,
+       Source/Vidyut.cpp:146-186): ions and neutrals solved in chunks of
+       comp_ion_chunks / comp_neutral_chunks consecutive components, each
+       chunk as one multigrid solve whose stopping test and bottom BiCGStab
+       inner products run over all of its components; background species in
+       the neutral range take part and are then reset to the step's starting
+       value (defaults: off, chunks NUM_IONS and NUM_NEUTRALS) */
+    int multicompsolves;
+    int comp_ion_chunks;
+    int comp_neutral_chunks;
 } vd_config;
 
 typedef struct vd_case_info_t {
@@ -253,6 +264,18 @@ vd_status vd_explicit_rhs(void* ctx, double time, double* expl_src, int on_devic
 vd_status vd_implicit_diffusion(void* ctx, int specid, double time,
                                 const double* expl_src, int on_device,
                                 vd_solve_stats* stats);
+
+/* Vidyut::implicit_solve_scalar with numspec > 1 (Source/ScalarSolve.cpp:
+ * 380-1000, as Source/Evolve.cpp:458-533 calls it for a chunk of ions or
+ * neutrals): species [startspec, startspec + numspec) solved together, one
+ * multigrid solve whose stopping test (max-norm) and bottom BiCGStab inner
+ * products run over all of them; writes every species of the chunk (floored
+ * like the reference).  numspec = 1 is vd_implicit_diffusion.  Chunks of
+ * more than one species need a 3-D non-periodic grid whose coarsest level
+ * holds at most 32 cells (VD_ERR_UNSUPPORTED otherwise). */
+vd_status vd_implicit_diffusion_chunk(void* ctx, int startspec, int numspec, double time,
+                                      const double* expl_src, int on_device,
+                                      vd_solve_stats* stats);
 
 /* Count of non-finite values in the species, energy and potential
  * components (a host-side check in place of amrex::Abort on NaN). */

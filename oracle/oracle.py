@@ -42,6 +42,8 @@ def load(case: str) -> C.CDLL:
         "vdo_poisson_solve": [P, C.c_double, C.POINTER(vb.vd_solve_stats)],
         "vdo_explicit_rhs": [P, C.c_double, P],
         "vdo_implicit_diffusion": [P, C.c_int, C.c_double, P, C.POINTER(vb.vd_solve_stats)],
+        "vdo_implicit_diffusion_chunk": [P, C.c_int, C.c_int, C.c_double, P,
+                                         C.POINTER(vb.vd_solve_stats)],
         "vdo_adjoint_tlm": [P, C.c_int, C.POINTER(C.c_double), C.c_int,
                             C.POINTER(C.c_double), C.POINTER(C.c_double), P],
     }
@@ -120,6 +122,14 @@ class Oracle:
         a = np.ascontiguousarray(expl_src, dtype=np.float64)
         st = vb.vd_solve_stats()
         self.lib.vdo_implicit_diffusion(self.ctx, specid, time, _ptr(a), C.byref(st))
+        return st
+
+    def implicit_solve_chunk(self, startspec: int, numspec: int, expl_src: np.ndarray,
+                             time: float = 0.0, allow_unconverged: bool = True):
+        a = np.ascontiguousarray(expl_src, dtype=np.float64)
+        st = vb.vd_solve_stats()
+        self.lib.vdo_implicit_diffusion_chunk(self.ctx, startspec, numspec, time, _ptr(a),
+                                              C.byref(st))
         return st
 
     def adjoint_tlm(self, nsteps: int, params, species: bool = False):

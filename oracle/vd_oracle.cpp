@@ -554,7 +554,9 @@ struct OMG
         return 8;
     }
 
-    void vcycle()
+    // A V-cycle on the correction equation in three parts, so that a
+    // multicomponent solve can run its bottom solve jointly.
+    void vcycle_down()
     {
         const int nl = (int)L.size();
         for (int l = 0; l < nl - 1; ++l)
@@ -564,23 +566,31 @@ struct OMG
             residual(l, L[l].cor, L[l].res, L[l].rescor, false);
             restrict_to(l, L[l].rescor, L[l + 1].res);
         }
-        {
-            const int l = nl - 1;
-            if (nl == 1)
-            {
-                for (int s = 0; s < nuf; ++s) smooth(l, L[l].cor, L[l].res, false);
-            } else
-            {
-                const int ret = bicgstab(l, L[l].cor, L[l].res);
-                const int ns = (ret == 0) ? nub : nuf;
-                for (int s = 0; s < ns; ++s) smooth(l, L[l].cor, L[l].res, false);
-            }
-        }
+    }
+    // smoothing of the bottom level after its BiCGStab returned `ret`
+    void bottom_smooth(int ret)
+    {
+        const int l = (int)L.size() - 1;
+        const int ns = (L.size() == 1) ? nuf : ((ret == 0) ? nub : nuf);
+        for (int s = 0; s < ns; ++s) smooth(l, L[l].cor, L[l].res, false);
+    }
+    void vcycle_up()
+    {
+        const int nl = (int)L.size();
         for (int l = nl - 2; l >= 0; --l)
         {
             prolong_add(l, L[l].cor, L[l + 1].cor);
             for (int s = 0; s < nu2; ++s) smooth(l, L[l].cor, L[l].res, false);
         }
+    }
+
+    void vcycle()
+    {
+        const int nl = (int)L.size();
+        vcycle_down();
+        const int ret = (nl == 1) ? 0 : bicgstab(nl - 1, L[nl - 1].cor, L[nl - 1].res);
+        bottom_smooth(ret);
+        vcycle_up();
     }
 
     // Build the level hierarchy: halve every active direction while it stays
@@ -810,6 +820,153 @@ struct OMG
         }
     }
 };
+
+// --- multicomponent solve (MLMG with ncomp > 1, Source/ScalarSolve.cpp:
+// 540-875 called with numspec > 1 by Source/Evolve.cpp:458-573) -----------
+// The components share one operator shape but have their own coefficients,
+// boundary data and right-hand sides; smoothing, restriction and
+// prolongation act on each component alone, while the stopping test uses
+// the max-norm over all components (MLMG's ResNormInf over ncomp) and the
+// bottom BiCGStab's inner products sum over all components (MLCGSolver's
+// dot products over ncomp), so its scalars rho, alpha, omega are shared.
+
+// Joint BiCGStab on the bottom level l of every component.
+int bicgstab_joint(std::vector<OMG*>& ms, int l)
+{
+    const size_t nc = ms.size();
+    const Geom& g = ms[0]->L[l].geo;
+    const long long n = g.ncell();
+    std::vector<std::vector<Real>> r(nc), rh(nc), p(nc), v(nc), sv(nc), t(nc);
+    for (size_t m = 0; m < nc; ++m)
+    {
+        auto& x = ms[m]->L[l].cor;
+        std::fill(x.begin(), x.end(), 0.0);
+        r[m] = ms[m]->L[l].res;
+        rh[m] = r[m];
+        p[m].assign(n, 0.0);
+        v[m].assign(n, 0.0);
+        sv[m].assign(n, 0.0);
+        t[m].assign(n, 0.0);
+    }
+    auto ninf = [&](std::vector<std::vector<Real>>& a) {
+        Real mx = 0.0;
+        for (size_t m = 0; m < nc; ++m) mx = std::max(mx, OMG::norminf(a[m]));
+        return mx;
+    };
+    auto dot = [&](std::vector<std::vector<Real>>& a, std::vector<std::vector<Real>>& b) {
+        Real acc = 0.0;
+        for (size_t m = 0; m < nc; ++m)
+        {
+            Real pm = 0.0;
+            for (long long q = 0; q < n; ++q) pm += a[m][q] * b[m][q];
+            acc += pm;
+        }
+        return acc;
+    };
+    auto apply = [&](std::vector<std::vector<Real>>& in, std::vector<std::vector<Real>>& out) {
+        for (size_t m = 0; m < nc; ++m)
+            for (int k = 0; k < g.n[2]; ++k)
+                for (int j = 0; j < g.n[1]; ++j)
+                    for (int i = 0; i < g.n[0]; ++i)
+                        out[m][OMG::idx(g, i, j, k)] = ms[m]->Lx(l, in[m], i, j, k, false);
+    };
+    const Real rnorm0 = ninf(r);
+    if (rnorm0 == 0.0) return 0;
+    const Real rel = ms[0]->bot_rel;
+    Real rho_1 = 0, alpha_ = 0, omega = 0;
+    for (int iter = 1; iter <= ms[0]->bot_maxiter; ++iter)
+    {
+        const Real rho = dot(rh, r);
+        if (rho == 0.0) return 1;
+        if (iter == 1)
+            p = r;
+        else
+        {
+            const Real bet = (rho / rho_1) * (alpha_ / omega);
+            for (size_t m = 0; m < nc; ++m)
+                for (long long q = 0; q < n; ++q) p[m][q] = r[m][q] + bet * (p[m][q] - omega * v[m][q]);
+        }
+        apply(p, v);
+        const Real rhTv = dot(rh, v);
+        if (rhTv == 0.0) return 2;
+        alpha_ = rho / rhTv;
+        for (size_t m = 0; m < nc; ++m)
+            for (long long q = 0; q < n; ++q)
+            {
+                ms[m]->L[l].cor[q] += alpha_ * p[m][q];
+                sv[m][q] = r[m][q] - alpha_ * v[m][q];
+            }
+        if (ninf(sv) <= rel * rnorm0) return 0;
+        apply(sv, t);
+        const Real tt = dot(t, t);
+        if (tt == 0.0) return 3;
+        omega = dot(t, sv) / tt;
+        for (size_t m = 0; m < nc; ++m)
+            for (long long q = 0; q < n; ++q)
+            {
+                ms[m]->L[l].cor[q] += omega * sv[m][q];
+                r[m][q] = sv[m][q] - omega * t[m][q];
+            }
+        if (ninf(r) <= rel * rnorm0) return 0;
+        if (omega == 0.0) return 4;
+        rho_1 = rho;
+    }
+    return 8;
+}
+
+// Joint solve of L_m(sol_m) = rhs_m, m = 0..nc-1; returns the V-cycles, -1
+// when maxiter is hit.
+int joint_solve(std::vector<OMG*>& ms, std::vector<std::vector<Real>*>& sol,
+                std::vector<std::vector<Real>>& rhs, Real tol_rel, Real tol_abs, vd_solve_stats* st)
+{
+    const size_t nc = ms.size();
+    Real r0 = 0.0, b0 = 0.0;
+    for (size_t m = 0; m < nc; ++m)
+    {
+        ms[m]->apply_inhomog_neumann(rhs[m]);
+        ms[m]->residual(0, *sol[m], rhs[m], ms[m]->L[0].res, true);
+        r0 = std::max(r0, OMG::norminf(ms[m]->L[0].res));
+        b0 = std::max(b0, OMG::norminf(rhs[m]));
+    }
+    const Real target = std::max(tol_abs, std::max(tol_rel, 1e-16) * std::max(b0, r0));
+    if (st)
+    {
+        st->initial_residual = r0;
+        st->final_residual = r0;
+        st->iterations = 0;
+        st->converged = 1;
+    }
+    if (r0 <= target) return 0;
+    const int nl = (int)ms[0]->L.size();
+    for (int it = 1; it <= ms[0]->maxiter; ++it)
+    {
+        for (auto* m : ms)
+        {
+            std::fill(m->L[0].cor.begin(), m->L[0].cor.end(), 0.0);
+            m->vcycle_down();
+        }
+        const int ret = (nl == 1) ? 0 : bicgstab_joint(ms, nl - 1);
+        Real rn = 0.0;
+        for (size_t m = 0; m < nc; ++m)
+        {
+            ms[m]->bottom_smooth(ret);
+            ms[m]->vcycle_up();
+            auto& x = *sol[m];
+            for (size_t q = 0; q < x.size(); ++q) x[q] += ms[m]->L[0].cor[q];
+            ms[m]->residual(0, x, rhs[m], ms[m]->L[0].res, true);
+            rn = std::max(rn, OMG::norminf(ms[m]->L[0].res));
+        }
+        if (st)
+        {
+            st->final_residual = rn;
+            st->iterations = it;
+        }
+        if (rn <= target) return it;
+    }
+    if (st) st->converged = 0;
+    return -1;
+}
+
 
 } // namespace
 
@@ -1265,17 +1422,30 @@ void elecenergy_source(OCtx& c, Fab& Sborder, Fab& rxn, FaceFab* efield,
 }
 
 // --- implicit_solve_scalar (Source/ScalarSolve.cpp:380-1000) -------------
-void implicit_solve(OCtx& c, Real time, Real dt, int spec, Fab& Sborder,
-                    Fab& Sborder_old, Fab& expl, const int* bclo, const int* bchi,
-                    FaceFab* grad_out, vd_solve_stats* st)
+// One species' (or the electron energy's) implicit-diffusion system,
+// set up (operator, boundary data, scaled right-hand side and initial
+// guess) apart from its solve, so that several can be solved jointly.
+struct SpecSolve
+{
+    int spec = 0;
+    bool is_e = false, is_een = false;
+    Real scale = 1.0;
+    OMG mg;
+    std::vector<Real> rhs, sol;
+};
+
+void species_setup(OCtx& c, Real time, Real dt, int spec, Fab& Sborder, Fab& Sborder_old,
+                   Fab& expl, const int* bclo, const int* bchi, SpecSolve& S)
 {
     const Geom& geo = c.geo;
     const vd_config& cfg = c.cfg;
-    const bool is_e = (spec == c.E_IDX);
-    const bool is_een = (spec == EEN_ID);
+    S.spec = spec;
+    S.is_e = (spec == c.E_IDX);
+    S.is_een = (spec == EEN_ID);
     const Real ts = cfg.time_scale;
-    const Real scale = is_een ? cfg.elecenergy_scale : cfg.species_scale[spec];
-    OMG mg;
+    const Real scale = S.is_een ? cfg.elecenergy_scale : cfg.species_scale[spec];
+    S.scale = scale;
+    OMG& mg = S.mg;
     mg.dim = geo.dim;
     mg.maxorder = 3;
     mg.alpha = 1.0;
@@ -1290,7 +1460,10 @@ void implicit_solve(OCtx& c, Real time, Real dt, int spec, Fab& Sborder,
     Array4 sbo = Sborder_old.view();
     const Real Tg = cfg.gas_temperature, Pg = cfg.gas_pressure;
 
-    std::vector<Real> rhs(N), sol(N);
+    std::vector<Real>& rhs = S.rhs;
+    std::vector<Real>& sol = S.sol;
+    rhs.assign(N, 0.0);
+    sol.assign(N, 0.0);
     // acoeff = 1/dt * timescale; rhs = (1/dt) n_old + S_expl, scaled
 #pragma omp parallel for collapse(2)
     for (int k = 0; k < geo.n[2]; ++k)
@@ -1378,9 +1551,21 @@ void implicit_solve(OCtx& c, Real time, Real dt, int spec, Fab& Sborder,
         mg.L[0].rb[s] = bd.rb[s];
     }
     mg.average_down_coeffs();
-    const int it = mg.solve(sol, rhs, cfg.linsolve_reltol, cfg.linsolve_abstol, st);
-    if (it > 0) c.n_species_iters += it;
-    if (it < 0) c.n_species_iters += cfg.linsolve_maxiter;
+}
+
+// Scale the solution back, floor it and copy it into phi_new (and the
+// electron temperature from a solved energy); the electrons' face gradient
+// for the Joule heating.
+void species_finish(OCtx& c, Fab& Sborder, SpecSolve& S, FaceFab* grad_out)
+{
+    const Geom& geo = c.geo;
+    const vd_config& cfg = c.cfg;
+    Array4 sb = Sborder.view();
+    const bool is_e = S.is_e, is_een = S.is_een;
+    const Real scale = S.scale;
+    const int spec = S.spec;
+    OMG& mg = S.mg;
+    std::vector<Real>& sol = S.sol;
     if (is_e && grad_out)
     {
         mg.grad(sol, grad_out);
@@ -1421,6 +1606,18 @@ void implicit_solve(OCtx& c, Real time, Real dt, int spec, Fab& Sborder,
                     }
                 }
     }
+}
+
+void implicit_solve(OCtx& c, Real time, Real dt, int spec, Fab& Sborder,
+                    Fab& Sborder_old, Fab& expl, const int* bclo, const int* bchi,
+                    FaceFab* grad_out, vd_solve_stats* st)
+{
+    SpecSolve S;
+    species_setup(c, time, dt, spec, Sborder, Sborder_old, expl, bclo, bchi, S);
+    const int it = S.mg.solve(S.sol, S.rhs, c.cfg.linsolve_reltol, c.cfg.linsolve_abstol, st);
+    if (it > 0) c.n_species_iters += it;
+    if (it < 0) c.n_species_iters += c.cfg.linsolve_maxiter;
+    species_finish(c, Sborder, S, grad_out);
 }
 
 // --- compute_electemp_lfa (Source/ElecEnergySource.cpp:17-70) ------------
@@ -1513,6 +1710,96 @@ void compute_dt(OCtx& c)
         c.cfg.dt = c.fixed_dt;
 }
 
+// --- multicomponent species solves (Source/Evolve.cpp:458-573) ----------
+// Chunk sizes after the reference's checks (Source/Vidyut.cpp:146-186): a
+// Robin wall forces chunks of one.  The reference tests lo[0], hi[0], then
+// lo[1] and lo[2] twice each (never hi[1], hi[2]); restated as it reads.
+void multicomp_chunks(const vd_config& cfg, int& ion_chunk, int& neutral_chunk)
+{
+    ion_chunk = cfg.comp_ion_chunks;
+    neutral_chunk = cfg.comp_neutral_chunks;
+    auto robin = [&](const int* lo, const int* hi) {
+        bool r = lo[0] == ROBINBC || hi[0] == ROBINBC;
+        if (cfg.dim > 1) r = r || lo[1] == ROBINBC || lo[1] == ROBINBC;
+        if (cfg.dim > 2) r = r || lo[2] == ROBINBC || lo[2] == ROBINBC;
+        return r;
+    };
+    if (robin(cfg.ion_bc_lo, cfg.ion_bc_hi)) ion_chunk = 1;
+    if (robin(cfg.neutral_bc_lo, cfg.neutral_bc_hi)) neutral_chunk = 1;
+}
+
+// [first, first+num) in chunks of `chunk`, then the remainder
+// (Source/Evolve.cpp:462-495).
+std::vector<std::pair<int, int>> chunk_list(int first, int num, int chunk)
+{
+    std::vector<std::pair<int, int>> out;
+    if (num <= 0 || chunk <= 0) return out;
+    int comp = first;
+    for (; comp <= first + num - chunk; comp += chunk) out.push_back({comp, chunk});
+    if (comp != first + num) out.push_back({comp, first + num - comp});
+    return out;
+}
+
+void multicomp_species(OCtx& c, Real t, Real dt, Fab& Sborder, Fab& Sborder_old, Fab& rxn,
+                       Fab& expl)
+{
+    const Geom& geo = c.geo;
+    const vd_config& cfg = c.cfg;
+    int ich, nch;
+    multicomp_chunks(cfg, ich, nch);
+    auto run = [&](int first, int num, int chunk, const int* lo, const int* hi) {
+        for (auto ch : chunk_list(first, num, chunk))
+        {
+            expl.setVal(0.0);
+            for (int sp = ch.first; sp < ch.first + ch.second; ++sp)
+                update_explsrc(c, sp, lo, hi, Sborder, rxn, expl, t);
+            if (ch.second == 1)
+            {
+                implicit_solve(c, t, dt, ch.first, Sborder, Sborder_old, expl, lo, hi, nullptr,
+                               nullptr);
+                continue;
+            }
+            std::vector<SpecSolve> ss(ch.second);
+            std::vector<OMG*> ms;
+            std::vector<std::vector<Real>*> sols;
+            std::vector<std::vector<Real>> rhs;
+            for (int q = 0; q < ch.second; ++q)
+            {
+                species_setup(c, t, dt, ch.first + q, Sborder, Sborder_old, expl, lo, hi, ss[q]);
+                ms.push_back(&ss[q].mg);
+                sols.push_back(&ss[q].sol);
+                rhs.push_back(ss[q].rhs);
+            }
+            const int it = joint_solve(ms, sols, rhs, cfg.linsolve_reltol, cfg.linsolve_abstol,
+                                       nullptr);
+            c.n_species_iters += (it >= 0) ? it : cfg.linsolve_maxiter;
+            for (auto& S : ss) species_finish(c, Sborder, S, nullptr);
+        }
+    };
+    if (NUM_IONS > 0) run(FIRST_ION, NUM_IONS, ich, cfg.ion_bc_lo, cfg.ion_bc_hi);
+    if (NUM_NEUTRALS > 0)
+        run(FIRST_NEUTRAL, NUM_NEUTRALS, nch, cfg.neutral_bc_lo, cfg.neutral_bc_hi);
+    // background species: back to the step's starting value, then their
+    // reactions (Source/Evolve.cpp:534-572)
+    for (int sp = 0; sp < NUM_SPECIES; ++sp)
+    {
+        if (!is_bg(c, sp)) continue;
+        for (int k = 0; k < geo.n[2]; ++k)
+            for (int j = 0; j < geo.n[1]; ++j)
+                for (int i = 0; i < geo.n[0]; ++i)
+                {
+                    Real& v = c.phi_new(i, j, k, sp);
+                    v = c.phi_old(i, j, k, sp);
+                    if (cfg.do_bg_reactions)
+                    {
+                        v += rxn(i, j, k, sp) * dt;
+                        if (v < cfg.min_species_density && cfg.bound_specden)
+                            v = cfg.min_species_density;
+                    }
+                }
+    }
+}
+
 // --- one coarse step (Source/Evolve.cpp:136-617) -------------------------
 void evolve_one(OCtx& c)
 {
@@ -1588,6 +1875,16 @@ void evolve_one(OCtx& c)
                            c.cfg.eenrg_bc_hi, nullptr, nullptr);
         }
         if (c.cfg.using_LFA) electemp_lfa(c, Sborder);
+        if (c.cfg.multicompsolves)
+        {
+            multicomp_species(c, t, dt, Sborder, Sborder_old, rxn, expl);
+            if (niter < ncorr - 1)
+            {
+                for (size_t q = 0; q < c.phi_new.d.size(); ++q)
+                    c.phi_new.d[q] = 0.5 * c.phi_old.d[q] + 0.5 * c.phi_new.d[q];
+            }
+            continue;
+        }
         for (int sp = 0; sp < NUM_SPECIES; ++sp)
         {
             const bool bgs = is_bg(c, sp);
@@ -1795,6 +2092,36 @@ int vdo_implicit_diffusion(void* ctx, int spec, double time, const double* expl_
     implicit_solve(*c, time, c->cfg.dt, spec, Sb, Sb, expl, bc_lo_for(*c, spec),
                    bc_hi_for(*c, spec), nullptr, st);
     return VD_OK;
+}
+
+// Species [start, start + num) solved jointly (implicit_solve_scalar with
+// numspec = num), each with its own boundary codes.
+int vdo_implicit_diffusion_chunk(void* ctx, int start, int num, double time,
+                                 const double* expl_in, vd_solve_stats* st)
+{
+    auto* c = static_cast<OCtx*>(ctx);
+    if (num < 1 || start < 0 || start + num > NUM_SPECIES) return VD_ERR_INVALID_ARG;
+    if (num == 1) return vdo_implicit_diffusion(ctx, start, time, expl_in, st);
+    Fab Sb, expl;
+    Sb.define(c->geo, NVAR, c->ngrow);
+    expl.define(c->geo, NUM_SPECIES + 1, 0);
+    fill_patch(c->geo, c->phi_new, Sb, NVAR);
+    std::memcpy(expl.d.data(), expl_in, sizeof(double) * expl.d.size());
+    std::vector<SpecSolve> ss(num);
+    std::vector<OMG*> ms;
+    std::vector<std::vector<Real>*> sols;
+    std::vector<std::vector<Real>> rhs;
+    for (int q = 0; q < num; ++q)
+    {
+        species_setup(*c, time, c->cfg.dt, start + q, Sb, Sb, expl, bc_lo_for(*c, start + q),
+                      bc_hi_for(*c, start + q), ss[q]);
+        ms.push_back(&ss[q].mg);
+        sols.push_back(&ss[q].sol);
+        rhs.push_back(ss[q].rhs);
+    }
+    const int it = joint_solve(ms, sols, rhs, c->cfg.linsolve_reltol, c->cfg.linsolve_abstol, st);
+    for (auto& S : ss) species_finish(*c, Sb, S, nullptr);
+    return it >= 0 ? VD_OK : VD_ERR_NOT_CONVERGED;
 }
 
 } // extern "C"

@@ -69,6 +69,8 @@ class vd_config(C.Structure):
         ("num_bg_species", C.c_int), ("bg_species_ids", C.c_int * VD_MAX_SPECIES),
         ("mg_precision", C.c_int), ("mg_inner_cycles", C.c_int),
         ("poisson_warm_start", C.c_int), ("device", C.c_int),
+        ("multicompsolves", C.c_int), ("comp_ion_chunks", C.c_int),
+        ("comp_neutral_chunks", C.c_int),
     ]
 
 
@@ -103,6 +105,7 @@ EXPORTS = [
     "vd_step", "vd_poisson_solve", "vd_explicit_rhs", "vd_implicit_diffusion",
     "vd_check_state", "vd_launch_count", "vd_profile_kernel", "vd_profile_read",
     "vd_last_error", "vd_poisson_solve_noalloc", "vd_adjoint_num_params",
+    "vd_implicit_diffusion_chunk",
     "vd_adjoint_set_params", "vd_adjoint_forward", "vd_adjoint_run",
 ]
 
@@ -152,6 +155,8 @@ def load(case: str) -> C.CDLL:
         "vd_poisson_solve": [P, C.c_double, C.POINTER(vd_solve_stats)],
         "vd_explicit_rhs": [P, C.c_double, P, C.c_int],
         "vd_implicit_diffusion": [P, C.c_int, C.c_double, P, C.c_int, C.POINTER(vd_solve_stats)],
+        "vd_implicit_diffusion_chunk": [P, C.c_int, C.c_int, C.c_double, P, C.c_int,
+                                        C.POINTER(vd_solve_stats)],
         "vd_check_state": [P, C.POINTER(C.c_longlong)],
         "vd_launch_count": [P, C.POINTER(C.c_longlong)],
         "vd_profile_kernel": [P, C.c_int],
@@ -360,6 +365,18 @@ class Vidyut:
             r = self.lib.vd_implicit_diffusion(self.ctx, specid, time, _ptr(a), 0, C.byref(st))
         if not (allow_unconverged and r == 3):
             self._chk(r, "vd_implicit_diffusion")
+        return st
+
+    def implicit_solve_chunk(self, startspec: int, numspec: int, expl_src: np.ndarray,
+                             time: float = 0.0, allow_unconverged: bool = False) -> vd_solve_stats:
+        """Species [startspec, startspec + numspec) solved together
+        (vd_implicit_diffusion_chunk)."""
+        a = np.ascontiguousarray(expl_src, dtype=np.float64)
+        st = vd_solve_stats()
+        r = self.lib.vd_implicit_diffusion_chunk(self.ctx, startspec, numspec, time, _ptr(a), 0,
+                                                 C.byref(st))
+        if not (allow_unconverged and r == 3):
+            self._chk(r, "vd_implicit_diffusion_chunk")
         return st
 
     def check_state(self) -> int:

@@ -27,6 +27,13 @@ struct CudaError
 {
     std::string msg;
     explicit CudaError(std::string m) : msg(std::move(m)) {}
+    virtual ~CudaError() = default;
+};
+
+// A request the library does not support (returned as VD_ERR_UNSUPPORTED).
+struct UnsupportedError : CudaError
+{
+    explicit UnsupportedError(std::string m) : CudaError(std::move(m)) {}
 };
 
 // Grid of one multigrid level (or of the state): cell counts, active

@@ -405,6 +405,10 @@ struct ExplParams
     int bchi[VD_NT][3];
     int bg[NUM_SPECIES];
     const ProbParm* pp;
+    // multicomponent solves: background species' pure reaction sources,
+    // slot bgslot[sp] of rxn_bg (null otherwise)
+    double* rxn_bg;
+    int bgslot[NUM_SPECIES];
 };
 
 __device__ __forceinline__ bool wall_zero(int code) { return code == IHNEUBC || code == AXISBC; }
@@ -656,7 +660,11 @@ __global__ void __launch_bounds__(256, EX_MINB) k_explicit_stream(ExplParams P, 
                 if (P.rxn_e) P.rxn_e[t] = rxa[P.eidx];
 #pragma unroll
                 for (int sp = 0; sp < NUM_SPECIES; sp++)
-                    if (P.bg[sp]) P.expl[sp * N + t] = P.do_bg_rxn ? rxa[sp] : 0.0;
+                    if (P.bg[sp])
+                    {
+                        P.expl[sp * N + t] = P.do_bg_rxn ? rxa[sp] : 0.0;
+                        if (P.rxn_bg) P.rxn_bg[P.bgslot[sp] * N + t] = rxa[sp];
+                    }
                 // reaction sources of components handled by later group launches
                 for (int q = EX_QB; q < P.ntr; ++q)
                 {
@@ -1035,6 +1043,12 @@ struct FinalParams
     int do_bg_rxn;
     double dt;
     GridDev gm; // layout of the solve outputs u[]
+    // multicomponent solves (Source/Evolve.cpp:534-572): background species
+    // go back to the step's starting value Sold, and their reactions use the
+    // pure reaction source rxn_bg (slot bgslot[sp]); otherwise null
+    const double* Sold;
+    const double* rxn_bg;
+    int bgslot[NUM_SPECIES];
 };
 
 __global__ void k_finalize(FinalParams P)
@@ -1069,10 +1083,14 @@ __global__ void k_finalize(FinalParams P)
             S[c * N + t] = v;
         }
         for (int sp = 0; sp < NUM_SPECIES; sp++)
-            if (P.bg[sp] && P.do_bg_rxn)
+            if (P.bg[sp] && (P.do_bg_rxn || P.Sold))
             {
-                double v = S[sp * N + t] + P.expl[sp * N + t] * P.dt;
-                if (v < P.min_s && P.bound_specden) v = P.min_s;
+                double v = P.Sold ? P.Sold[sp * N + t] : S[sp * N + t];
+                if (P.do_bg_rxn)
+                {
+                    v += (P.rxn_bg ? P.rxn_bg[P.bgslot[sp] * N + t] : P.expl[sp * N + t]) * P.dt;
+                    if (v < P.min_s && P.bound_specden) v = P.min_s;
+                }
                 S[sp * N + t] = v;
             }
         const double ne_new = S[P.eidx * N + t];

@@ -474,24 +474,42 @@ void bottom(Hier<T>& H, const MGOp<T>& op, T* x, const T* f, cudaStream_t st)
 
 // One V-cycle on x0.  With nf given, its first level-0 sweep also takes the
 // convergence norm of x0 as it was on entry (NormFuse).
+// First level small enough for the one-CTA coarse cycle (never level 0).
 template <typename T>
-void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaStream_t st,
-            const NormFuse* nf = nullptr)
+int vcycle_lc(const Hier<T>& H)
 {
     const int L = H.nlev;
-    if (L == 1)
-    {
-        const Grid3 gn = rows3(H.g[0], 8);
-        LAUNCH(k_mg_resid_norm<T>, gn.g, gn.b, st, H.op[0], x0, f0, H.t0f, dscr, inh0 ? 1 : 0,
-               0, 8, (double*)nullptr);
-        bottom(H, H.op[0], H.t0x, H.t0f, st);
-        LAUNCH(k_add_same<T>, gsz(H.g[0].ncell()), BS, st, x0, H.t0x, H.g[0].ncell(),
-               H.op[0].stop);
-        return;
-    }
-    // first level small enough for the one-CTA coarse cycle (never level 0)
     int lc = L - 1;
     while (lc > 1 && H.g[lc - 1].ncell() <= VD_MG_ONCHIP_CELLS) --lc;
+    return lc;
+}
+
+// Whether the coarse levels from lc run as k_mg_coarse3 (3-D, non-periodic,
+// on chip).
+template <typename T>
+bool coarse3_ok(const Hier<T>& H, int lc, size_t* smem = nullptr)
+{
+    MGCoarse<T> C{};
+    C.lc = lc;
+    C.nl = H.nlev;
+    bool c3 = true;
+    for (int l = lc; l < H.nlev; ++l)
+    {
+        const GridDev& g = H.g[l];
+        C.op[l] = H.op[l];
+        c3 = c3 && g.dim == 3 && !g.per[0] && !g.per[1] && !g.per[2] && !H.op[l].a &&
+             g.n[0] < 1024 && g.n[1] < 1024 && g.n[2] < 1024;
+    }
+    const size_t smem3 = mg_coarse3_smem(C);
+    if (smem) *smem = smem3;
+    return c3 && smem3 <= VD_MG_COARSE_SMEM;
+}
+
+// The levels above the coarse cycle, going down: smoothing and restriction.
+template <typename T>
+void vcycle_down(Hier<T>& H, T* x0, T* f0, bool inh0, cudaStream_t st, const NormFuse* nf,
+                 int lc)
+{
     for (int l = 0; l < lc; ++l)
     {
         T* xl = l ? H.x[l] : x0;
@@ -520,47 +538,58 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
         LAUNCH_PDL(k_mg_resid_restrict<T>, gr.g, gr.b, st, H.op[l], xl, fl, H.g[l + 1], H.f[l + 1],
                H.x[l + 1], inh ? 1 : 0);
     }
-    if (lc == L - 1)
-        bottom(H, H.op[L - 1], H.x[L - 1], H.f[L - 1], st);
-    else
+}
+
+template <typename T>
+MGCoarse<T> coarse_of(const Hier<T>& H, int lc)
+{
+    MGCoarse<T> C{};
+    C.lc = lc;
+    C.nl = H.nlev;
+    for (int l = lc; l < H.nlev; ++l)
     {
-        MGCoarse<T> C{};
-        C.lc = lc;
-        C.nl = L;
-        for (int l = lc; l < L; ++l)
-        {
-            C.op[l] = H.op[l];
-            C.x[l] = H.x[l];
-            C.f[l] = H.f[l];
-        }
-        // levels on chip when they fit (vd_create raises the kernel's dynamic
-        // shared-memory limit to VD_MG_COARSE_SMEM)
-        bool c3 = true; // all coarse levels 3-D, non-periodic, on chip
-        for (int l = lc; l < L; ++l)
-        {
-            const GridDev& g = H.g[l];
-            c3 = c3 && g.dim == 3 && !g.per[0] && !g.per[1] && !g.per[2] && !H.op[l].a &&
-                 g.n[0] < 1024 && g.n[1] < 1024 && g.n[2] < 1024;
-        }
-        const size_t smem3 = mg_coarse3_smem(C);
-        if (c3 && smem3 <= VD_MG_COARSE_SMEM)
-        {
-            if (H.varb)
-                launch_pdl(k_mg_coarse3<T, true>, dim3(1), dim3(MGC_THREADS), smem3, st, C,
-                           T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf);
-            else
-                launch_pdl(k_mg_coarse3<T, false>, dim3(1), dim3(MGC_THREADS), smem3, st, C,
-                           T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf);
-        } else
-        {
-            const size_t smem = mg_coarse_smem(C);
-            const int on_chip = smem <= VD_MG_COARSE_SMEM ? 1 : 0;
-            k_mg_coarse_vcycle<T><<<1, 512, on_chip ? smem : 0, st>>>(
-                C, H.scratch, T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf, on_chip);
-            ++vd::g_launches;
-            VD_CUDA_OK(cudaGetLastError());
-        }
+        C.op[l] = H.op[l];
+        C.x[l] = H.x[l];
+        C.f[l] = H.f[l];
     }
+    return C;
+}
+
+// The coarse levels lc .. nl-1 of one component.
+template <typename T>
+void vcycle_coarse(Hier<T>& H, cudaStream_t st, int lc)
+{
+    const int L = H.nlev;
+    if (lc == L - 1)
+    {
+        bottom(H, H.op[L - 1], H.x[L - 1], H.f[L - 1], st);
+        return;
+    }
+    const MGCoarse<T> C = coarse_of(H, lc);
+    size_t smem3 = 0;
+    if (coarse3_ok(H, lc, &smem3))
+    {
+        if (H.varb)
+            launch_pdl(k_mg_coarse3<T, true>, dim3(1), dim3(MGC_THREADS), smem3, st, C,
+                       T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf);
+        else
+            launch_pdl(k_mg_coarse3<T, false>, dim3(1), dim3(MGC_THREADS), smem3, st, C,
+                       T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf);
+    } else
+    {
+        const size_t smem = mg_coarse_smem(C);
+        const int on_chip = smem <= VD_MG_COARSE_SMEM ? 1 : 0;
+        k_mg_coarse_vcycle<T><<<1, 512, on_chip ? smem : 0, st>>>(
+            C, H.scratch, T(H.bot_rel), H.bot_maxiter, H.nu1, H.nu2, H.nub, H.nuf, on_chip);
+        ++vd::g_launches;
+        VD_CUDA_OK(cudaGetLastError());
+    }
+}
+
+// The levels above the coarse cycle, going up: prolongation and smoothing.
+template <typename T>
+void vcycle_up(Hier<T>& H, T* x0, T* f0, bool inh0, cudaStream_t st, int lc)
+{
     for (int l = lc - 1; l >= 0; --l)
     {
         T* xl = l ? H.x[l] : x0;
@@ -587,6 +616,27 @@ void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaS
                H.op[l].stop);
         smooth(H.op[l], xl, fl, inh, H.nu2, st, l == 0 ? H.prof_tag : VD_PROF_NONE);
     }
+}
+
+template <typename T>
+void vcycle(Hier<T>& H, T* x0, T* f0, bool inh0, unsigned long long* dscr, cudaStream_t st,
+            const NormFuse* nf = nullptr)
+{
+    const int L = H.nlev;
+    if (L == 1)
+    {
+        const Grid3 gn = rows3(H.g[0], 8);
+        LAUNCH(k_mg_resid_norm<T>, gn.g, gn.b, st, H.op[0], x0, f0, H.t0f, dscr, inh0 ? 1 : 0,
+               0, 8, (double*)nullptr);
+        bottom(H, H.op[0], H.t0x, H.t0f, st);
+        LAUNCH(k_add_same<T>, gsz(H.g[0].ncell()), BS, st, x0, H.t0x, H.g[0].ncell(),
+               H.op[0].stop);
+        return;
+    }
+    const int lc = vcycle_lc(H);
+    vcycle_down(H, x0, f0, inh0, st, nf, lc);
+    vcycle_coarse(H, st, lc);
+    vcycle_up(H, x0, f0, inh0, st, lc);
 }
 
 // ------------------------------------------------------------ context
@@ -641,7 +691,48 @@ struct Ctx
     int not_converged = 0;
     double max_poisson_res = 0.0;
     struct AdjState* adjs = nullptr; // discrete-adjoint buffers, made on first use
+    // multicomponent species solves: effective chunk sizes and, per chunk
+    // slot, a species hierarchy, boundary arrays and a right-hand side
+    int ion_chunk = 1, neutral_chunk = 1;
+    std::vector<Hier<double>> HJ;
+    std::vector<std::array<SideArrays, 6>> JS;
+    std::vector<double*> JR;
+    MGCoarse<double>* dcoarse = nullptr; // per-slot coarse-cycle descriptors
+    MGCoarse<double>* hcoarse = nullptr; // pinned staging copy
+    double* rxn_bg = nullptr;            // background species' reaction sources
+    int bgslot[NUM_SPECIES] = {};
 };
+
+// Effective multicomponent chunk sizes (Source/Vidyut.cpp:146-186): a Robin
+// species wall forces chunks of one.  The reference tests lo[0], hi[0], then
+// lo[1] twice and lo[2] twice (never hi[1], hi[2]); restated as it reads.
+void multicomp_chunks(const vd_config& cfg, int& ion_chunk, int& neutral_chunk)
+{
+    ion_chunk = cfg.comp_ion_chunks;
+    neutral_chunk = cfg.comp_neutral_chunks;
+    auto robin = [&](const int* lo, const int* hi) {
+        bool r = lo[0] == ROBINBC || hi[0] == ROBINBC;
+        if (cfg.dim > 1) r = r || lo[1] == ROBINBC || lo[1] == ROBINBC;
+        if (cfg.dim > 2) r = r || lo[2] == ROBINBC || lo[2] == ROBINBC;
+        return r;
+    };
+    if (robin(cfg.ion_bc_lo, cfg.ion_bc_hi)) ion_chunk = 1;
+    if (robin(cfg.neutral_bc_lo, cfg.neutral_bc_hi)) neutral_chunk = 1;
+}
+
+// [first, first + num) in chunks of `chunk`, then the remainder
+// (Source/Evolve.cpp:462-495).
+std::vector<std::pair<int, int>> chunk_list(int first, int num, int chunk)
+{
+    std::vector<std::pair<int, int>> out;
+    if (num <= 0 || chunk <= 0) return out;
+    int comp = first;
+    for (; comp <= first + num - chunk; comp += chunk) out.push_back({comp, chunk});
+    if (comp != first + num) out.push_back({comp, first + num - comp});
+    return out;
+}
+
+bool in_neutral_range(int sp) { return sp >= FIRST_NEUTRAL && sp < FIRST_NEUTRAL + NUM_NEUTRALS; }
 
 std::string g_create_err;
 
@@ -1133,11 +1224,16 @@ void explicit_rhs(Ctx& c, double time, int qlo = 0, int qhi = 1 << 30)
     P.do_reactions = cfg.do_reactions;
     P.do_bg_rxn = cfg.do_bg_reactions;
     P.pp = c.dpp;
+    P.rxn_bg = c.rxn_bg;
     int n = 0;
     for (int sp = 0; sp < NUM_SPECIES; ++sp)
     {
         P.bg[sp] = c.bg[sp];
-        if (c.bg[sp]) continue;
+        P.bgslot[sp] = c.bgslot[sp];
+        // multicomponent solves take the background species of the neutral
+        // range into their chunk (Source/Evolve.cpp:496-533): they need
+        // their explicit source like any transported species
+        if (c.bg[sp] && !(cfg.multicompsolves && in_neutral_range(sp))) continue;
         P.comp[n] = sp;
         for (int d = 0; d < 3; ++d)
         {
@@ -1178,7 +1274,13 @@ void explicit_rhs(Ctx& c, double time, int qlo = 0, int qhi = 1 << 30)
 }
 
 // ---- implicit_solve_scalar (Source/ScalarSolve.cpp:380-858)
-void species_solve(Ctx& c, int comp, double time, const double* Sold, vd_solve_stats* stats)
+// FP64 set-up of one species' (or the electron energy's) system into a
+// hierarchy H with boundary arrays `sides` and right-hand side `rhs`: face
+// diffusivities, scaled right-hand side and initial guess (the current
+// state), boundary data from the species_bc hook, operators, coarse
+// coefficients, inhomogeneous-Neumann adjustment.
+void species_setup64(Ctx& c, int comp, double time, const double* Sold, Hier<double>& H,
+                     SideArrays* sides, double* rhs)
 {
     const vd_config& cfg = c.cfg;
     const double ts = cfg.time_scale;
@@ -1186,12 +1288,24 @@ void species_solve(Ctx& c, int comp, double time, const double* Sold, vd_solve_s
     const int* bct = bct_for(c, comp);
     for (int d = 0; d < cfg.dim; ++d)
         LAUNCH(k_species_faces, gsz(face_count(c.g, d)), BS, c.st, c.g, d, c.S, comp,
-               cfg.gas_temperature, c.HS.bf[0][d]);
-    LAUNCH(k_species_rhs, gsz(c.N), BS, c.st, c.g, c.HS.g[0], c.S, Sold, c.expl, comp, cfg.dt,
-           ts, scale, c.spec_rhs, c.u[comp]);
-    fill_bc(c, 1, comp, bct, 3, 1.0 / scale, time, c.sside);
-    hier_set_ops(c.HS, (1.0 / cfg.dt) * ts * 1.0, ts, 1.0, bct, 3);
-    hier_coarsen_coeffs(c.HS, bct, c.st);
+               cfg.gas_temperature, H.bf[0][d]);
+    LAUNCH(k_species_rhs, gsz(c.N), BS, c.st, c.g, H.g[0], c.S, Sold, c.expl, comp, cfg.dt,
+           ts, scale, rhs, c.u[comp]);
+    fill_bc(c, 1, comp, bct, 3, 1.0 / scale, time, sides);
+    hier_set_ops(H, (1.0 / cfg.dt) * ts * 1.0, ts, 1.0, bct, 3);
+    hier_coarsen_coeffs(H, bct, c.st);
+    for (int s = 0; s < 6; ++s)
+        if (bct[s] == MG_INNEU)
+            LAUNCH(k_inneu_adjust, gsz(plane_count(c.g, s % 3)), BS, c.st, H.g[0], s,
+                   (const double*)H.bf[0][s % 3], 1.0, ts, c.G.dx[s % 3], sides[s].val, rhs);
+}
+
+void species_solve(Ctx& c, int comp, double time, const double* Sold, vd_solve_stats* stats)
+{
+    const vd_config& cfg = c.cfg;
+    const double ts = cfg.time_scale;
+    const int* bct = bct_for(c, comp);
+    species_setup64(c, comp, time, Sold, c.HS, c.sside, c.spec_rhs);
     if (cfg.mg_precision == VD_MG_FP32_REFINED)
     {
         for (int d = 0; d < cfg.dim; ++d)
@@ -1204,11 +1318,6 @@ void species_solve(Ctx& c, int comp, double time, const double* Sold, vd_solve_s
         hier_set_ops(c.HS32, (1.0 / cfg.dt) * ts * 1.0, ts, 1.0, bct, 3);
         hier_coarsen_coeffs(c.HS32, bct, c.st);
     }
-    for (int s = 0; s < 6; ++s)
-        if (bct[s] == MG_INNEU)
-            LAUNCH(k_inneu_adjust, gsz(plane_count(c.g, s % 3)), BS, c.st, c.HS.g[0], s,
-                   (const double*)c.HS.bf[0][s % 3], 1.0, ts, c.G.dx[s % 3], c.sside[s].val,
-                   c.spec_rhs);
     vd_solve_stats st{};
     // species solves run in FP64 unless the last one needed more than two
     // V-cycles: the implicit-diffusion operator is strongly diagonal (one
@@ -1220,6 +1329,94 @@ void species_solve(Ctx& c, int comp, double time, const double* Sold, vd_solve_s
     const int it = mg_solve(c, c.HS, c.HS32, c.u[comp], c.spec_rhs, &st, c.hint[comp], allow32);
     if (st.converged && it > 0) c.hint[comp] = it;
     c.species_iters += it;
+    if (stats) *stats = st;
+}
+
+// One multicomponent solve of species [first, first + nc) (MLMG with
+// ncomp = nc, Source/ScalarSolve.cpp:540-875): each component is set up in
+// its own chunk slot and smoothed, restricted and prolonged on its own; the
+// stopping test takes the max-norm over all components and the bottom
+// BiCGStab runs jointly in a thread-block cluster of nc CTAs
+// (k_mg_coarse3_joint).  FP64 in both precision forms.  Cycles are enqueued
+// one at a time with the joint norm read back after each.
+void joint_solve(Ctx& c, int first, int nc, double time, const double* Sold,
+                 vd_solve_stats* stats)
+{
+    const vd_config& cfg = c.cfg;
+    if (nc > (int)c.HJ.size())
+        throw CudaError("multicomponent chunk larger than the slots made at vd_create");
+    for (int q = 0; q < nc; ++q)
+    {
+        species_setup64(c, first + q, time, Sold, c.HJ[q], c.JS[q].data(), c.JR[q]);
+        for (auto& o : c.HJ[q].op) o.stop = nullptr;
+    }
+    Hier<double>& H0 = c.HJ[0];
+    const int lc = vcycle_lc(H0);
+    size_t smem3 = 0;
+    if (H0.nlev < 2 || lc == H0.nlev - 1 || !coarse3_ok(H0, lc, &smem3) ||
+        H0.g[H0.nlev - 1].ncell() > 32)
+        throw UnsupportedError("multicomponent solves of more than one component need a 3-D, "
+                               "non-periodic grid whose coarsest multigrid level holds at most "
+                               "32 cells");
+    auto norms = [&](double* bmax) {
+        double r = 0.0, b = 0.0;
+        for (int q = 0; q < nc; ++q)
+        {
+            double bq = 0.0;
+            const double rq = resid_norm(c, c.HJ[q].op[0], (const double*)c.u[first + q],
+                                         (const double*)c.JR[q], (double*)nullptr, true,
+                                         bmax ? &bq : nullptr);
+            r = std::max(r, rq);
+            b = std::max(b, bq);
+        }
+        if (bmax) *bmax = b;
+        return r;
+    };
+    double b0 = 0.0;
+    const double r0 = norms(&b0);
+    const double target =
+        std::max(cfg.linsolve_abstol, std::max(cfg.linsolve_reltol, 1e-16) * std::max(b0, r0));
+    vd_solve_stats st{};
+    st.initial_residual = st.final_residual = r0;
+    st.converged = r0 <= target;
+    if (!st.converged)
+    {
+        for (int q = 0; q < nc; ++q) c.hcoarse[q] = coarse_of(c.HJ[q], lc);
+        VD_CUDA_OK(cudaMemcpyAsync(c.dcoarse, c.hcoarse, nc * sizeof(MGCoarse<double>),
+                                   cudaMemcpyHostToDevice, c.st));
+        for (int it = 1; it <= cfg.linsolve_maxiter; ++it)
+        {
+            for (int q = 0; q < nc; ++q)
+                vcycle_down(c.HJ[q], c.u[first + q], c.JR[q], true, c.st, nullptr, lc);
+            cudaLaunchConfig_t lcfg{};
+            lcfg.gridDim = dim3(nc);
+            lcfg.blockDim = dim3(MGC_THREADS);
+            lcfg.dynamicSmemBytes = smem3;
+            lcfg.stream = c.st;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = nc;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            lcfg.attrs = at;
+            lcfg.numAttrs = 1;
+            VD_CUDA_OK(cudaLaunchKernelEx(&lcfg, k_mg_coarse3_joint<double, true>,
+                                          (const MGCoarse<double>*)c.dcoarse, H0.bot_rel,
+                                          H0.bot_maxiter, H0.nu1, H0.nu2, H0.nub, H0.nuf));
+            ++vd::g_launches;
+            for (int q = 0; q < nc; ++q)
+                vcycle_up(c.HJ[q], c.u[first + q], c.JR[q], true, c.st, lc);
+            st.iterations = it;
+            st.final_residual = norms(nullptr);
+            if (st.final_residual <= target)
+            {
+                st.converged = 1;
+                break;
+            }
+        }
+    }
+    c.species_iters += st.iterations;
+    if (!st.converged) c.not_converged++;
     if (stats) *stats = st;
 }
 
@@ -1269,6 +1466,30 @@ void add_solved(Ctx& c, FinalParams& P, int comp)
     P.scale[P.nsol] = (comp == EEN_ID) ? c.cfg.elecenergy_scale : c.cfg.species_scale[comp];
     P.nsol++;
 }
+
+// The species solves of one corrector iteration with multicompsolves: ions
+// then neutrals in chunks (Source/Evolve.cpp:458-533); background species
+// take part and their solutions are dropped (k_finalize resets them).
+void multicomp_species(Ctx& c, FinalParams& P, double t, const double* Sold)
+{
+    auto run = [&](int first, int num, int chunk) {
+        for (const auto& ch : chunk_list(first, num, chunk))
+        {
+            if (ch.second == 1)
+                species_solve(c, ch.first, t, Sold, nullptr);
+            else
+                joint_solve(c, ch.first, ch.second, t, Sold, nullptr);
+            for (int q = 0; q < ch.second; ++q)
+                if (!c.bg[ch.first + q]) add_solved(c, P, ch.first + q);
+        }
+    };
+    if (NUM_IONS > 0) run(FIRST_ION, NUM_IONS, c.ion_chunk);
+    if (NUM_NEUTRALS > 0) run(FIRST_NEUTRAL, NUM_NEUTRALS, c.neutral_chunk);
+    P.Sold = Sold;
+    P.rxn_bg = c.rxn_bg;
+    for (int sp = 0; sp < NUM_SPECIES; ++sp) P.bgslot[sp] = c.bgslot[sp];
+}
+
 
 // ---- one coarse step (Source/Evolve.cpp:136-617)
 // ---- find_time_scales + ComputeDt (Source/TimeStep.cpp:14-134): the
@@ -1359,12 +1580,15 @@ void step_once(Ctx& c)
             P.heat_diag = 1;
         }
         P.lfa = cfg.using_LFA;
-        for (int sp = 0; sp < NUM_SPECIES; ++sp)
-        {
-            if (c.bg[sp] || sp == c.eidx) continue;
-            species_solve(c, sp, t, Sold, nullptr);
-            add_solved(c, P, sp);
-        }
+        if (cfg.multicompsolves)
+            multicomp_species(c, P, t, Sold);
+        else
+            for (int sp = 0; sp < NUM_SPECIES; ++sp)
+            {
+                if (c.bg[sp] || sp == c.eidx) continue;
+                species_solve(c, sp, t, Sold, nullptr);
+                add_solved(c, P, sp);
+            }
         P.do_bg_rxn = cfg.do_bg_reactions;
         LAUNCH(k_finalize, gsz(c.N), BS, c.st, P);
         if (niter < ncorr - 1)
@@ -1456,6 +1680,8 @@ const Key g_keys[] = {
     KD("vidyut.time_scale", time_scale), KI("vidyut.mg_precision", mg_precision),
     KI("vidyut.mg_inner_cycles", mg_inner_cycles),
     KI("vidyut.poisson_warm_start", poisson_warm_start), KI("vidyut.device", device),
+    KI("vidyut.multicompsolves", multicompsolves), KI("vidyut.comp_ion_chunks", comp_ion_chunks),
+    KI("vidyut.comp_neutral_chunks", comp_neutral_chunks),
 };
 
 
@@ -1717,6 +1943,9 @@ vd_status vd_config_init(vd_config* c)
     for (int i = 0; i < VD_MAX_SPECIES; ++i) c->species_scale[i] = 1.0;
     c->mg_precision = VD_MG_FP64;
     c->mg_inner_cycles = 2;
+    c->multicompsolves = 0;
+    c->comp_ion_chunks = NUM_IONS;
+    c->comp_neutral_chunks = NUM_NEUTRALS;
     return VD_OK;
 }
 
@@ -1895,8 +2124,9 @@ vd_status vd_create(const vd_config* cfg, void** out)
         VD_CUDA_OK(cudaMemset(c->expl, 0, sizeof(double) * (size_t)VD_NT * N));
         c->rxn_een = c->A.get<double>(N);
         c->ejh = c->A.get<double>(N);
-        for (int sp = 0; sp < NUM_SPECIES; ++sp)
-            if (!c->bg[sp]) c->u[sp] = c->A.get<double>(N);
+        // a solution array per species (background ones too: a
+        // multicomponent chunk or vd_implicit_diffusion_chunk may solve them)
+        for (int sp = 0; sp < NUM_SPECIES; ++sp) c->u[sp] = c->A.get<double>(N);
         c->u[EEN_ID] = c->A.get<double>(N);
         c->phi_sol = c->A.get<double>(N);
         c->phi_rhs = c->A.get<double>(N);
@@ -1929,10 +2159,67 @@ vd_status vd_create(const vd_config* cfg, void** out)
             hier_build(c->HS32, c->A, g, dx, mcl, true, true);
             c->r64 = c->A.get<double>(N);
         }
+        // multicomponent species solves: one slot per component of the
+        // largest chunk, and the background species' reaction sources
+        multicomp_chunks(*cfg, c->ion_chunk, c->neutral_chunk);
+        if (cfg->multicompsolves && (c->ion_chunk < 1 || c->neutral_chunk < 1))
+            throw UnsupportedError("comp_ion_chunks and comp_neutral_chunks must be at least 1");
+        {
+            int maxk = 1;
+            if (cfg->multicompsolves)
+            {
+                for (const auto& ch : chunk_list(FIRST_ION, NUM_IONS, c->ion_chunk))
+                    maxk = std::max(maxk, ch.second);
+                for (const auto& ch : chunk_list(FIRST_NEUTRAL, NUM_NEUTRALS, c->neutral_chunk))
+                    maxk = std::max(maxk, ch.second);
+            }
+            if (maxk > 8)
+                throw UnsupportedError("multicomponent chunks hold at most 8 components (one "
+                                       "thread-block cluster of the joint bottom solve)");
+            // vd_implicit_diffusion_chunk can ask for chunks in any mode
+            maxk = std::max(maxk, std::min(8, std::max(NUM_IONS, NUM_NEUTRALS)));
+            if (maxk > 1)
+            {
+                c->HJ.resize(maxk);
+                c->JS.resize(maxk);
+                c->JR.resize(maxk);
+                for (int q = 0; q < maxk; ++q)
+                {
+                    for (int s = 0; s < 6; ++s)
+                    {
+                        const int np = plane_count(g, s % 3);
+                        SideArrays* sa = &c->JS[q][s];
+                        sa->val = c->A.get<double>(np);
+                        sa->ra = c->A.get<double>(np);
+                        sa->rb = c->A.get<double>(np);
+                        sa->rf = c->A.get<double>(np);
+                        sa->g = c->A.get<double>(np);
+                        sa->c0 = c->A.get<double>(np);
+                    }
+                    c->JR[q] = c->A.get<double>(N);
+                }
+                c->dcoarse = c->A.get<MGCoarse<double>>(maxk);
+                VD_CUDA_OK(cudaMallocHost(&c->hcoarse, maxk * sizeof(MGCoarse<double>)));
+            }
+        }
+        if (cfg->multicompsolves)
+        {
+            int nbg = 0;
+            for (int sp = 0; sp < NUM_SPECIES; ++sp)
+                if (c->bg[sp]) c->bgslot[sp] = nbg++;
+            if (nbg) c->rxn_bg = c->A.get<double>((size_t)nbg * N);
+        }
         if (cfg->poisson_warm_start)
         {
             c->zero64 = c->A.get<double>(N);
             VD_CUDA_OK(cudaMemset(c->zero64, 0, sizeof(double) * (size_t)N));
+        }
+        for (size_t q = 0; q < c->HJ.size(); ++q)
+        {
+            hier_build(c->HJ[q], c->A, g, dx, mcl, true, false);
+            bind_sides64(c->HJ[q], c->JS[q].data());
+            c->HJ[q].nu1 = cfg->linsolve_num_pre_smooth;
+            c->HJ[q].nu2 = cfg->linsolve_num_post_smooth;
         }
         for (Hier<double>* h : {&c->HP, &c->HS})
         {
@@ -1946,6 +2233,7 @@ vd_status vd_create(const vd_config* cfg, void** out)
         }
         for (const void* kf : {(const void*)k_mg_coarse3<double, false>,
                                (const void*)k_mg_coarse3<double, true>,
+                               (const void*)k_mg_coarse3_joint<double, true>,
                                (const void*)k_mg_coarse3<float, false>,
                                (const void*)k_mg_coarse3<float, true>})
             VD_CUDA_OK(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1977,10 +2265,12 @@ vd_status vd_create(const vd_config* cfg, void** out)
         VD_CUDA_OK(cudaDeviceSynchronize());
     } catch (const CudaError& e)
     {
+        const bool unsup = dynamic_cast<const UnsupportedError*>(&e) != nullptr;
         g_create_err = e.msg;
         c->A.release();
+        if (c->hcoarse) cudaFreeHost(c->hcoarse);
         delete c;
-        return VD_ERR_CUDA;
+        return unsup ? VD_ERR_UNSUPPORTED : VD_ERR_CUDA;
     }
     *out = c;
     return VD_OK;
@@ -2000,6 +2290,7 @@ vd_status vd_destroy(void* ctx)
     if (c->hscal) cudaFreeHost(c->hscal);
     if (c->hmg) cudaFreeHost(c->hmg);
     if (c->hts) cudaFreeHost(c->hts);
+    if (c->hcoarse) cudaFreeHost(c->hcoarse);
     delete c->adjs;
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -2015,6 +2306,10 @@ vd_status vd_destroy(void* ctx)
         VD_CUDA_OK(cudaSetDevice(c->dev));                                       \
         body;                                                                    \
         VD_CUDA_OK(cudaStreamSynchronize(c->st));                                \
+    } catch (const UnsupportedError& e)                                          \
+    {                                                                            \
+        c->err = e.msg;                                                          \
+        return VD_ERR_UNSUPPORTED;                                               \
     } catch (const CudaError& e)                                                 \
     {                                                                            \
         c->err = e.msg;                                                          \
@@ -2191,6 +2486,26 @@ vd_status vd_implicit_diffusion(void* ctx, int spec, double time, const double* 
         FinalParams P = final_params(*c);
         add_solved(*c, P, spec);
         P.een_solved = (spec == EEN_ID) ? 1 : 0;
+        LAUNCH(k_finalize, gsz(c->N), BS, c->st, P);
+    });
+    return c->not_converged ? VD_ERR_NOT_CONVERGED : VD_OK;
+}
+
+vd_status vd_implicit_diffusion_chunk(void* ctx, int startspec, int numspec, double time,
+                                      const double* expl_in, int on_device,
+                                      vd_solve_stats* stats)
+{
+    if (!ctx || !expl_in || numspec < 1 || startspec < 0) return VD_ERR_INVALID_ARG;
+    if (numspec == 1) return vd_implicit_diffusion(ctx, startspec, time, expl_in, on_device, stats);
+    if (startspec + numspec > NUM_SPECIES) return VD_ERR_INVALID_ARG;
+    VD_TRY({
+        c->not_converged = 0;
+        VD_CUDA_OK(cudaMemcpyAsync(c->expl, expl_in, sizeof(double) * (size_t)VD_NT * c->N,
+                                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                   c->st));
+        joint_solve(*c, startspec, numspec, time, c->S, stats);
+        FinalParams P = final_params(*c);
+        for (int q = 0; q < numspec; ++q) add_solved(*c, P, startspec + q);
         LAUNCH(k_finalize, gsz(c->N), BS, c->st, P);
     });
     return c->not_converged ? VD_ERR_NOT_CONVERGED : VD_OK;

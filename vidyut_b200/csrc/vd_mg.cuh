@@ -19,6 +19,7 @@
 #pragma once
 
 #include "vd_common.cuh"
+#include <cooperative_groups.h>
 #include <vector>
 
 
@@ -2193,11 +2194,163 @@ __device__ void mgc_bottom_warp(const MGOp<T>& L, const MGCLevel<T> V, T* __rest
         }
 }
 
+// Joint bottom solve of a multicomponent system (MLMG with ncomp > 1):
+// each CTA of a thread-block cluster holds one component's bottom level
+// (at most 32 cells, in warp 0), and every inner product and max-norm of
+// BiCGStab is reduced over the whole cluster through distributed shared
+// memory, so the Krylov scalars rho, alpha, omega are those of the joint
+// system (MLCGSolver's dot products run over all components).  Every CTA
+// forms the same sums (partials added in rank order), so all take the same
+// branches and the same number of cluster barriers.  Partials go to one of
+// two slots per CTA by the parity of the reduction's sequence number: a
+// slot is rewritten two reductions later, after a barrier that every
+// reader of its previous value has passed.  All threads of the CTA call
+// this; threads past warp 0 hold no cells.
 template <typename T, bool VARB>
-__global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3(MGCoarse<T> C, T rel, int maxiter,
-                                                            int nu1, int nu2, int nub, int nuf)
+__device__ void mgc_bottom_joint(const MGOp<T>& L, const MGCLevel<T> V, T* __restrict__ scr,
+                                 T rel, int maxiter, int nub, int nuf)
 {
-    VD_PDL_WAIT();
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned nblk = cl.num_blocks();
+    __shared__ T red[2];
+    const unsigned FULL = 0xffffffffu;
+    const int n = (int)L.g.ncell();
+    const bool w0 = threadIdx.x < 32;
+    const int lane = threadIdx.x & 31;
+    const bool act = w0 && lane < n;
+    const int nx = L.g.n[0], ny = L.g.n[1];
+    const int c = act ? lane : 0;
+    const int i = c % nx, rr = c / nx, j = rr % ny, k = rr / ny;
+    T w[6], G;
+    int o[6];
+    mgc_weights<T, VARB>(L, i, j, k, w, o, G);
+    T* p = scr;
+    T* sv = scr + n;
+    int seq = 0;
+    auto jred = [&](T v, bool mx) -> T {
+        if (w0)
+        {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1)
+            {
+                const T u = __shfl_xor_sync(FULL, v, off);
+                v = mx ? (u > v ? u : v) : v + u;
+            }
+            if (lane == 0) red[seq & 1] = v;
+        }
+        cl.sync();
+        T acc = T(0);
+        for (unsigned r = 0; r < nblk; ++r)
+        {
+            const T x = cl.map_shared_rank(red, r)[seq & 1];
+            acc = mx ? (x > acc ? x : acc) : acc + x;
+        }
+        ++seq;
+        return acc;
+    };
+    auto apply = [&](const T* u) {
+        T s = T(0);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) s += w[m] * u[c + o[m]];
+        return G * u[c] - s;
+    };
+    auto absv = [](T a) { return a < T(0) ? -a : a; };
+    T xv = T(0), rv = act ? V.f[c] : T(0);
+    const T rh = rv;
+    T pv = T(0), vv = T(0);
+    const T rnorm0 = jred(absv(rv), true);
+    int ret = 0;
+    if (rnorm0 > T(0))
+    {
+        ret = 8;
+        T rho_1 = T(1), alpha = T(1), omega = T(1);
+        for (int iter = 1; iter <= maxiter; ++iter)
+        {
+            const T rho = jred(rh * rv, false);
+            if (rho == T(0))
+            {
+                ret = 1;
+                break;
+            }
+            if (iter == 1)
+                pv = rv;
+            else
+            {
+                const T beta = (rho / rho_1) * (alpha / omega);
+                pv = rv + beta * (pv - omega * vv);
+            }
+            if (act) p[c] = pv;
+            __syncthreads();
+            vv = act ? apply(p) : T(0);
+            __syncthreads();
+            const T rhTv = jred(rh * vv, false);
+            if (rhTv == T(0))
+            {
+                ret = 2;
+                break;
+            }
+            alpha = rho / rhTv;
+            xv += alpha * pv;
+            const T sval = rv - alpha * vv;
+            if (jred(absv(sval), true) <= rel * rnorm0)
+            {
+                ret = 0;
+                break;
+            }
+            if (act) sv[c] = sval;
+            __syncthreads();
+            const T tv = act ? apply(sv) : T(0);
+            __syncthreads();
+            const T ttt = jred(tv * tv, false);
+            const T tts = jred(tv * sval, false);
+            if (ttt == T(0))
+            {
+                ret = 3;
+                break;
+            }
+            omega = tts / ttt;
+            xv += omega * sval;
+            rv = sval - omega * tv;
+            if (jred(absv(rv), true) <= rel * rnorm0)
+            {
+                ret = 0;
+                break;
+            }
+            if (omega == T(0))
+            {
+                ret = 4;
+                break;
+            }
+            rho_1 = rho;
+        }
+    }
+    // no CTA leaves while another may still read its partials
+    cl.sync();
+    if (act) V.x[c] = xv;
+    __syncthreads();
+    const int nsm = (ret == 0) ? nub : nuf;
+    for (int sm = 0; sm < nsm; ++sm)
+        for (int color = 0; color < 2; ++color)
+        {
+            if (act && ((i + j + k + color) & 1) == 0)
+            {
+                T s = T(0);
+#pragma unroll
+                for (int m = 0; m < 6; ++m) s += w[m] * V.x[c + o[m]];
+                V.x[c] = (V.f[c] + s) * V.iG[c];
+            }
+            __syncthreads();
+        }
+}
+
+// The coarse part of a V-cycle (levels lc .. nl-1) in one CTA, every level
+// in shared memory; JOINT: one component of a multicomponent system per CTA
+// of a cluster, with the bottom solve joint over the cluster.
+template <typename T, bool VARB, bool JOINT>
+__device__ __forceinline__ void mgc_run(const MGCoarse<T>& C, T rel, int maxiter, int nu1,
+                                        int nu2, int nub, int nuf)
+{
     extern __shared__ __align__(16) unsigned char mgc_smem[];
     __shared__ T sh[32];
     if (mg_stopped(C.op[C.lc])) return;
@@ -2292,7 +2445,9 @@ __global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3(MGCoarse<T> C, T rel
     {
         MGOp<T> Lb = C.op[last];
         Lb.g.rb = 0;
-        if (Lb.g.ncell() <= 32)
+        if constexpr (JOINT)
+            mgc_bottom_joint<T, VARB>(Lb, V[last], bscr, rel, maxiter, nub, nuf);
+        else if (Lb.g.ncell() <= 32)
         {
             if (threadIdx.x < 32) mgc_bottom_warp<T, VARB>(Lb, V[last], bscr, rel, maxiter, nub, nuf);
             __syncthreads();
@@ -2329,6 +2484,26 @@ __global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3(MGCoarse<T> C, T rel
             C.x[lc][L.g.idx(i, j, k)] = V[lc].x[i + nx * (j + ny * k)];
         }
     }
+}
+
+template <typename T, bool VARB>
+__global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3(MGCoarse<T> C, T rel, int maxiter,
+                                                            int nu1, int nu2, int nub, int nuf)
+{
+    VD_PDL_WAIT();
+    mgc_run<T, VARB, false>(C, rel, maxiter, nu1, nu2, nub, nuf);
+}
+
+// Multicomponent form: CTA b of a cluster of nc CTAs runs component b's
+// coarse cycle from Cs[b]; the bottom solve is joint over the cluster (the
+// host checks that the bottom level holds at most 32 cells).
+template <typename T, bool VARB>
+__global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse3_joint(const MGCoarse<T>* __restrict__ Cs,
+                                                                  T rel, int maxiter, int nu1,
+                                                                  int nu2, int nub, int nuf)
+{
+    VD_PDL_WAIT();
+    mgc_run<T, VARB, true>(Cs[blockIdx.x], rel, maxiter, nu1, nu2, nub, nuf);
 }
 
 // Shared memory of k_mg_coarse3 for levels lc .. nl-1.
