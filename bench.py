@@ -62,6 +62,20 @@ def load_traffic():
     return None
 
 
+def fp64_peak_gflops() -> float | None:
+    """FP64 FMA throughput of the current GPU (vidyut_b200/peak)."""
+    import ctypes
+    from vidyut_b200 import build
+    try:
+        lib = ctypes.CDLL(build.build_peak())
+        lib.vd_fp64_peak_gflops.restype = ctypes.c_double
+        lib.vd_fp64_peak_gflops.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        v = lib.vd_fp64_peak_gflops(8, 20000, 5)
+        return v if v > 0 else None
+    except Exception:
+        return None
+
+
 def cpu_model() -> str:
     try:
         with open("/proc/cpuinfo") as f:
@@ -495,6 +509,8 @@ def main():
     # first one's tail (programmatic dependent launch), which costs ~5 %
     # of the step.
     st_p, _, prof = timed(g, args.steps, dist, vb.VD_PROF_POISSON_SMOOTH)
+    # and once more with events around every explicit-source launch
+    _, _, prof_x = timed(g, args.steps, dist, vb.VD_PROF_EXPLICIT)
     clk = clocks.stop()
     ms_p = dist_max(dist, st_p.gpu_ms)
 
@@ -516,6 +532,27 @@ def main():
                     f"({ms_p / args.steps:.3f} ms/step under the events)",
             "traffic": (traffic or {}).get("bytes_per_launch") if traffic else None,
             "traffic_note": (traffic or {}).get("note") if traffic else None}
+
+    # the explicit kernel is FP64-arithmetic bound: its roofline is the FP64
+    # FLOP count per launch (ncu, committed under profiles/) over its
+    # per-launch device time, against the FP64 throughput measured here
+    fp64_peak = fp64_peak_gflops()
+    nx_l, xms, xbytes = prof_x
+    x_avg_s = (xms / nx_l) / 1e3 if nx_l else float("nan")
+    xflops = (traffic or {}).get("explicit_fp64_flops_per_launch")
+    roof_explicit = {
+        "kernel": "k_explicit_stream (fused reactions + WENO5-Z drift flux + divergence, one "
+                  "transported component per launch)",
+        "bound": "fp64", "unit": "GFLOP/s", "avg_launch_us": x_avg_s * 1e6 if nx_l else None,
+        "launches_timed": nx_l,
+        "flops_per_launch": xflops,
+        "achieved": (xflops / x_avg_s / 1e9) if (xflops and nx_l) else None,
+        "peak": fp64_peak, "peak_kind": "measured (vd_fp64_peak_gflops: FP64 FMA chains)",
+        "frac": (xflops / x_avg_s / 1e9 / fp64_peak) if (xflops and nx_l and fp64_peak) else None,
+        "hbm_achieved_gbs": xbytes / x_avg_s / 1e9 if nx_l else None,
+        "hbm_frac": (xbytes / x_avg_s / 1e9 / peak) if nx_l else None,
+        "algorithmic_bytes_per_launch": xbytes,
+        "flops_note": (traffic or {}).get("explicit_note")}
 
     if args.lean:
         if rank == 0:
@@ -590,6 +627,7 @@ def main():
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": roof,
+            "roofline_explicit": roof_explicit,
             "step_roofline": step_roofline(ms / args.steps, ncell, step_bytes(pv, sv, 2),
                                            peak, peak_kind),
             "cpu_baseline": cpu,

@@ -90,7 +90,31 @@ def build_host(case: str, force: bool = False) -> str:
     return out
 
 
+PEAK_SRC = os.path.join(PKG, "peak", "vd_fp64peak.cu")
+
+
+def peak_path() -> str:
+    return os.path.join(LIBDIR, "libvd_fp64peak.so")
+
+
+def build_peak(force: bool = False) -> str:
+    """The FP64 CUDA-core throughput probe (peak/vd_fp64peak.cu), the
+    denominator of the explicit kernel's roofline."""
+    os.makedirs(LIBDIR, exist_ok=True)
+    out = peak_path()
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(PEAK_SRC):
+        return out
+    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo",
+           "-Xcompiler", "-fPIC", "-shared", PEAK_SRC, "-o", out + ".tmp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for the FP64 probe:\n{r.stderr[-4000:]}")
+    os.replace(out + ".tmp", out)
+    return out
+
+
 def build_all(force: bool = False) -> list[str]:
+    build_peak(force)
     cs = cases()
     with ThreadPoolExecutor(max_workers=min(4, len(cs))) as ex:
         out = list(ex.map(lambda c: build_case(c, force), cs))
