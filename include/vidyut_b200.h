@@ -288,7 +288,9 @@ vd_status vd_launch_count(void* ctx, long long* launches);
  * around it on the context's stream, until the next vd_profile_kernel call;
  * vd_profile_read returns the launches timed, their summed device time and
  * the kernel's algorithmic bytes per launch (one read of each distinct input
- * array, one write of each output). */
+ * array, one write of each output); launches that returned at once on a
+ * solve's stop flag (a multigrid cycle enqueued past convergence; shorter
+ * than a quarter of the median launch) did no work and are left out. */
 vd_status vd_profile_kernel(void* ctx, int kernel_id);
 vd_status vd_profile_read(void* ctx, long long* launches, double* total_ms,
                           double* bytes_per_launch);

@@ -1034,18 +1034,11 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
             // cycle v+1 (NormFuse): the check lags one cycle, and a converged
             // solution carries one more colour-0 half-sweep than the cycles
             // counted
-            // A launch-by-launch timing pass (vd_profile_kernel) runs the
-            // cycles one at a time with the standalone norm, so that no
-            // cycle is enqueued past convergence and every timed sweep does
-            // its work (a sweep that returns at once on the stop flag would
-            // pull the per-launch average down); the V-cycles and results
-            // are the same.
-            const bool timing = t_prof && t_prof->id != VD_PROF_NONE;
             const bool fused = H64.nlev > 1 && H64.nu1 >= 1 && H64.nu2 >= 1 &&
-                               norm_fusable(op0, c.npart) && !timing;
+                               norm_fusable(op0, c.npart);
             const NormFuse nf{c.dpart, c.npart, c.dmg, target};
             int issued = 0;
-            int batch = timing ? 1 : fused ? hint + 1 : std::max(1, hint - 1);
+            int batch = fused ? hint + 1 : std::max(1, hint - 1);
             while (issued < cfg.linsolve_maxiter)
             {
                 const int nb = std::min(batch, cfg.linsolve_maxiter - issued);
@@ -1065,7 +1058,7 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
                 VD_CUDA_OK(cudaMemcpyAsync(c.hmg, c.dmg, sizeof(MGDev), cudaMemcpyDeviceToHost, c.st));
                 VD_CUDA_OK(cudaStreamSynchronize(c.st));
                 if (c.hmg->done) break;
-                batch = timing ? 1 : 2;
+                batch = 2;
             }
             if (fused && !c.hmg->done)
             {
@@ -2436,16 +2429,29 @@ vd_status vd_profile_read(void* ctx, long long* launches, double* total_ms,
                           double* bytes_per_launch)
 {
     double tot = 0.0;
+    long long used = 0;
     VD_TRY({
+        std::vector<float> t(c->prof.n);
         for (int i = 0; i < c->prof.n; ++i)
         {
-            float ms = 0.f;
             VD_CUDA_OK(cudaEventSynchronize(c->prof.b[i]));
-            VD_CUDA_OK(cudaEventElapsedTime(&ms, c->prof.a[i], c->prof.b[i]));
-            tot += ms;
+            VD_CUDA_OK(cudaEventElapsedTime(&t[i], c->prof.a[i], c->prof.b[i]));
         }
+        // V-cycles are enqueued in batches, and the launches of a cycle
+        // enqueued past convergence return at once on the stop flag (a few
+        // µs against tens for a working sweep): those did no work and are
+        // left out, by duration, below a quarter of the median launch
+        std::vector<float> srt = t;
+        std::sort(srt.begin(), srt.end());
+        const float cut = srt.empty() ? 0.f : 0.25f * srt[srt.size() / 2];
+        for (float ms : t)
+            if (ms >= cut)
+            {
+                tot += ms;
+                ++used;
+            }
     });
-    if (launches) *launches = c->prof.n;
+    if (launches) *launches = used;
     if (total_ms) *total_ms = tot;
     if (bytes_per_launch) *bytes_per_launch = c->prof.bytes;
     return VD_OK;
