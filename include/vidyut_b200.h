@@ -284,8 +284,11 @@ vd_status vd_check_state(void* ctx, long long* nonfinite);
 /* Per-kernel launch counter (for the benchmark's launch accounting). */
 vd_status vd_launch_count(void* ctx, long long* launches);
 
-/* Time every launch of one kernel (VD_PROF_*) with CUDA events recorded
- * around it on the context's stream, until the next vd_profile_kernel call;
+/* Time the launches of one kernel (VD_PROF_*) with CUDA events recorded on
+ * the context's stream, until the next vd_profile_kernel call (the
+ * multigrid sweeps: one event pair around each run of consecutive sweeps,
+ * so that the events do not break their programmatic overlap; the explicit
+ * kernel: one pair around the explicit stage of a step);
  * vd_profile_read returns the launches timed, their summed device time and
  * the kernel's algorithmic bytes per launch (one read of each distinct input
  * array, one write of each output); launches that returned at once on a

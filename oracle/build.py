@@ -38,6 +38,20 @@ def lib_path(case: str) -> str:
     return os.path.join(LIBDIR, f"liboracle_{case}.so")
 
 
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def _case_dir(case: str) -> str:
+    from vidyut_b200 import build as vbuild
+    return vbuild.case_dir(case)
+
+
+def _case_flags(case: str):
+    from vidyut_b200 import build as vbuild
+    return vbuild.case_flags(case)
+
+
 def _stale(case: str) -> bool:
     out = lib_path(case)
     if not os.path.exists(out):
@@ -46,7 +60,8 @@ def _stale(case: str) -> bool:
     deps = [os.path.join(HERE, "vd_oracle.cpp"), os.path.join(HERE, "oracle_defaults.H"),
             os.path.join(ROOT, "include", "vidyut_b200.h")]
     deps += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".H")]
-    deps += [os.path.join(CASES, case, f) for f in os.listdir(os.path.join(CASES, case))]
+    cdir = _case_dir(case)
+    deps += [os.path.join(cdir, f) for f in os.listdir(cdir)]
     return any(os.path.getmtime(p) > t for p in deps)
 
 
@@ -55,10 +70,10 @@ def build_case(case: str, force: bool = False) -> str:
     out = lib_path(case)
     if not force and not _stale(case):
         return out
+    inc, srcs = _case_flags(case)
     cmd = [CXX, "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
-           "-I", HERE, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           "-I", os.path.join(CASES, case),
-           os.path.join(HERE, "vd_oracle.cpp"), "-o", out + ".tmp"]
+           *inc, "-I", HERE, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+           os.path.join(HERE, "vd_oracle.cpp"), *srcs, "-o", out + ".tmp"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"g++ failed for oracle case {case}:\n{r.stderr[-6000:]}")

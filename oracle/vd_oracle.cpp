@@ -44,6 +44,7 @@
 #include <UserFunctions.H>
 #include <UserSources.H>
 #include <Prob.H>
+#include "vd_probinit.H"
 
 #include <algorithm>
 #include <cmath>
@@ -57,7 +58,19 @@ using vd::GpuArray;
 using vd::IntVect;
 using vd::Real;
 
+// A reference case directory's boundary hooks take three integrated-current
+// arrays more (vidyut_b200/compat defines them); otherwise nothing.
+#ifndef VD_CURRENT_ARGS
+#define VD_CURRENT_ARGS
+#endif
+
 namespace {
+using vd::Array4;
+using vd::Box;
+using vd::GeometryData;
+using vd::GpuArray;
+using vd::IntVect;
+using vd::Real;
 
 // ------------------------------------------------------------------ grids
 struct Geom
@@ -262,6 +275,23 @@ struct Side
     std::vector<Real> val, ra, rb, rf;
 };
 
+// Robin faces a*phi + b*dphi/dn = f on coarse levels.  Closed by the
+// two-point ghost over a cell of width h, a face passes the homogeneous flux
+// -kappa * phi_inside with the boundary conductance kappa = a / (a h/2 + b):
+// 2/h for Dirichlet, 0 for Neumann.  A coarse face (width H = 2h) keeps the
+// mean conductance of its fine faces, capped at its own Dirichlet value
+// 2/H, as the Dirichlet weight w = min(1, mean(kappa) H/2) stored as
+// (a, b) = (w, (1 - w) H/2) (conductance 2w/H).  Uniform Dirichlet and
+// Neumann sides coarsen to themselves exactly, a uniform weak Robin side
+// keeps its conductance, and Dirichlet patches in a Neumann wall keep
+// their share of the boundary flux; averaging a and b apart turns such a
+// wall nearly Neumann on the coarse levels, and the V-cycle then diverges.
+inline Real robin_conductance(Real a, Real b, Real h)
+{
+    const Real den = 0.5 * a * h + b;
+    return den != 0.0 ? a / den : 0.0;
+}
+
 struct OLevel
 {
     Geom geo;
@@ -453,12 +483,17 @@ struct OMG
         }
     }
 
+    // max |v|; a NaN entry reads as +inf, so a state that went non-finite
+    // never passes a convergence test
     static Real norminf(const std::vector<Real>& v)
     {
         Real m = 0.0;
 #pragma omp parallel for reduction(max : m)
         for (long long q = 0; q < (long long)v.size(); ++q)
-            m = std::max(m, std::fabs(v[q]));
+        {
+            const Real a = std::fabs(v[q]);
+            m = std::max(m, a == a ? a : HUGE_VAL);
+        }
         return m;
     }
 
@@ -683,7 +718,8 @@ struct OMG
                 for (int q = 0; q < na * nb; ++q)
                 {
                     const int ia = q % na, ib = q / na;
-                    Real sa = 0.0, sb = 0.0;
+                    const Real hf = gf.dx[d], hc = gc.dx[d];
+                    Real sk = 0.0;
                     int cnt = 0;
                     for (int u = 0; u < 2; ++u)
                         for (int w = 0; w < ((tb < dim) ? 2 : 1); ++w)
@@ -691,12 +727,12 @@ struct OMG
                             const int fa = 2 * ia + u;
                             const int fb = (tb < dim) ? 2 * ib + w : ib;
                             const int fp = fa + gf.n[ta] * fb;
-                            sa += L[l - 1].ra[s][fp];
-                            sb += L[l - 1].rb[s][fp];
+                            sk += robin_conductance(L[l - 1].ra[s][fp], L[l - 1].rb[s][fp], hf);
                             ++cnt;
                         }
-                    L[l].ra[s][q] = sa / cnt;
-                    L[l].rb[s][q] = sb / cnt;
+                    const Real w = std::min(1.0, (sk / cnt) * (0.5 * hc));
+                    L[l].ra[s][q] = w;
+                    L[l].rb[s][q] = (1.0 - w) * (0.5 * hc);
                 }
             }
         }
@@ -754,6 +790,11 @@ struct OMG
             st->final_residual = r0;
             st->iterations = 0;
             st->converged = 1;
+        }
+        if (!std::isfinite(r0))
+        {
+            if (st) st->converged = 0;
+            return -1;
         }
         if (r0 <= target) return 0;
         for (int it = 1; it <= maxiter; ++it)
@@ -989,6 +1030,12 @@ struct OCtx
 };
 
 namespace {
+using vd::Array4;
+using vd::Box;
+using vd::GeometryData;
+using vd::GpuArray;
+using vd::IntVect;
+using vd::Real;
 
 GpuArray<Real, 3> ga(const Real* v) { return GpuArray<Real, 3>{{v[0], v[1], v[2]}}; }
 
@@ -1171,7 +1218,7 @@ void solve_potential(OCtx& c, Real time, Fab& Sborder, Fab& Sborder_old,
             if (cfg.user_defined_potential)
                 user_transport::potential_bc(f[0], f[1], f[2], d, sgn, sb, bv, av, bbv, fv,
                                              plo, phi_, dx, time, c.pp, cfg.gas_temperature,
-                                             cfg.gas_pressure, app);
+                                             cfg.gas_pressure, app VD_CURRENT_ARGS);
             else
 #endif
                 plasmachem_transport::potential_bc(f[0], f[1], f[2], d, sgn, sb, bv, av, bbv,
@@ -1534,7 +1581,7 @@ void species_setup(OCtx& c, Real time, Real dt, int spec, Fab& Sborder, Fab& Sbo
 #ifdef VD_HAS_USER_TRANSPORT
             if (cfg.user_defined_species)
                 user_transport::species_bc(f[0], f[1], f[2], d, sgn, spec, 0, sb, bv, av, bbv, fv,
-                                           plo, phi_, dx, time, c.pp, Tg, Pg);
+                                           plo, phi_, dx, time, c.pp, Tg, Pg VD_CURRENT_ARGS);
             else
 #endif
                 plasmachem_transport::species_bc(f[0], f[1], f[2], d, sgn, spec, 0, sb, bv, av,
@@ -1972,10 +2019,8 @@ int vdo_destroy(void* ctx)
 int vdo_init_domain(void* ctx, const char* text)
 {
     auto* c = static_cast<OCtx*>(ctx);
-    auto table = vd::ParmParse::parse(text ? text : "");
-    vd::ParmParse pp(&table, "prob");
     c->pp = ProbParm{};
-    amrex_probinit(c->pp, pp);
+    vd_probinit(c->pp, text);
     vd::GeometryData gd;
     for (int d = 0; d < 3; ++d)
     {
@@ -1985,7 +2030,7 @@ int vdo_init_domain(void* ctx, const char* text)
         gd.n_cell[d] = c->geo.n[d];
     }
     vd::Box bx{{0, 0, 0}, {c->geo.n[0] - 1, c->geo.n[1] - 1, c->geo.n[2] - 1}};
-    Array4 v = c->phi_new.view();
+    vd::Array4 v = c->phi_new.view();
     initdomaindata(bx, v, gd, &c->pp);
     c->phi_old.d = c->phi_new.d;
     c->cur_time = 0.0;
@@ -1996,10 +2041,8 @@ int vdo_init_domain(void* ctx, const char* text)
 int vdo_set_probinit(void* ctx, const char* text)
 {
     auto* c = static_cast<OCtx*>(ctx);
-    auto table = vd::ParmParse::parse(text ? text : "");
-    vd::ParmParse pp(&table, "prob");
     c->pp = ProbParm{};
-    amrex_probinit(c->pp, pp);
+    vd_probinit(c->pp, text);
     return VD_OK;
 }
 
@@ -2139,6 +2182,12 @@ int vdo_implicit_diffusion_chunk(void* ctx, int start, int num, double time,
 #include "vd_dual.H"
 
 namespace {
+using vd::Array4;
+using vd::Box;
+using vd::GeometryData;
+using vd::GpuArray;
+using vd::IntVect;
+using vd::Real;
 
 constexpr int TLM_NP = NUM_REACTIONS + 1;
 using TD = vd::Dual<TLM_NP>;

@@ -250,6 +250,10 @@ class Config:
             if "=" not in line:
                 continue
             k, v = (s.strip() for s in line.split("=", 1))
+            if k == "amr.n_cell" and "dim" not in kw:
+                # the reference's dimension is a build switch; its inputs
+                # files give as many n_cell entries as it has dimensions
+                cfg["dim"] = 2 if len(v.split()) == 2 else 3
             try:
                 cfg.set(k, v)
             except VidyutError:

@@ -26,9 +26,53 @@ NVCC_FLAGS = [
 ]
 
 
+COMPAT = os.path.join(PKG, "compat")
+
+# case directories outside vidyut_b200/cases (register_case)
+EXTRA_CASES: dict[str, str] = {}
+
+
 def cases() -> list[str]:
     return sorted(d for d in os.listdir(CASES)
                   if os.path.isfile(os.path.join(CASES, d, "Chemistry.H")))
+
+
+def register_case(name: str, path: str) -> None:
+    """Build case `name` from the case directory at `path` (for example a
+    reference test/verification or test/models directory, compiled
+    unchanged through the compatibility headers in vidyut_b200/compat)."""
+    EXTRA_CASES[name] = os.path.abspath(path)
+
+
+def case_dir(case: str) -> str:
+    return EXTRA_CASES.get(case, os.path.join(CASES, case))
+
+
+def reference_style(cdir: str) -> bool:
+    """A case directory written against AMReX, as the reference's are (it
+    includes AMReX headers, and keeps species names in Chemistry.cpp)."""
+    if os.path.isfile(os.path.join(cdir, "Chemistry.cpp")):
+        return True
+    for f in os.listdir(cdir):
+        if f.endswith(".H"):
+            with open(os.path.join(cdir, f), errors="replace") as fh:
+                if "<AMReX_" in fh.read():
+                    return True
+    return False
+
+
+def case_flags(case: str) -> tuple[list[str], list[str]]:
+    """Include flags and extra sources of one case directory: a reference
+    case directory adds the compatibility headers and its Chemistry.cpp."""
+    cdir = case_dir(case)
+    inc = ["-I", cdir]
+    extra = []
+    if reference_style(cdir):
+        inc += ["-I", COMPAT]
+        cpp = os.path.join(cdir, "Chemistry.cpp")
+        if os.path.isfile(cpp):
+            extra.append(cpp)
+    return inc, extra
 
 
 def lib_path(case: str) -> str:
@@ -44,7 +88,9 @@ def _stale(case: str) -> bool:
     if not os.path.exists(out):
         return True
     t = os.path.getmtime(out)
-    deps = sources() + [os.path.join(CASES, case, f) for f in os.listdir(os.path.join(CASES, case))]
+    cdir = case_dir(case)
+    deps = sources() + [os.path.join(cdir, f) for f in os.listdir(cdir)]
+    deps += [os.path.join(COMPAT, f) for f in os.listdir(COMPAT)]
     deps.append(os.path.join(ROOT, "include", "vidyut_b200.h"))
     return any(os.path.getmtime(p) > t for p in deps)
 
@@ -54,10 +100,11 @@ def build_case(case: str, force: bool = False, extra: list[str] | None = None) -
     out = lib_path(case)
     if not force and not _stale(case):
         return out
-    cmd = [NVCC, *NVCC_FLAGS, *(extra or []),
-           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-I", os.path.join(CASES, case),
+    inc, srcs = case_flags(case)
+    cmd = [NVCC, *NVCC_FLAGS, *(extra or []), *inc,
+           "-I", os.path.join(ROOT, "include"), "-I", CSRC,
            f'-DVD_CASE_NAME="{case}"',
-           os.path.join(CSRC, "vd_lib.cu"), "-o", out + ".tmp"]
+           os.path.join(CSRC, "vd_lib.cu"), *srcs, "-o", out + ".tmp"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for case {case}:\n{r.stderr[-6000:]}")

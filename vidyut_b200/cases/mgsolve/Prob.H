@@ -1,10 +1,17 @@
 // The solver workload's state is generated on the host and copied in
 // (vidyut_b200/workloads.py, mgsolve_state); initdomaindata only clears it.
+// prob.* sets the electrode layout of the user potential callback.
 #pragma once
 #include "vd_vars.H"
 #include "vd_parmparse.H"
 
-inline void amrex_probinit(ProbParm& h_prob_parm, vd::ParmParse& pp) {}
+inline void amrex_probinit(ProbParm& h_prob_parm, vd::ParmParse& pp)
+{
+    pp.query("trode_rad", h_prob_parm.trode_rad);
+    pp.query("trode_sep", h_prob_parm.trode_sep);
+    pp.query("trode_volt", h_prob_parm.trode_volt);
+    pp.query("subs_rad", h_prob_parm.subs_rad);
+}
 
 AMREX_GPU_HOST_DEVICE AMREX_INLINE void initdomaindata(
     vd::Box const& bx, vd::Array4 const& phi, vd::GeometryData const& geomdata,

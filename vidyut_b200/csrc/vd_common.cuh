@@ -85,14 +85,19 @@ __device__ inline T warp_sum(T v)
     return v;
 }
 
+// Max that keeps a NaN: a residual norm taken over a state that went
+// non-finite must not read as converged (fmax and `a > m ? a : m` drop it).
+template <typename T>
+__host__ __device__ __forceinline__ T nanmax(T m, T a)
+{
+    return (a > m || a != a) ? a : m;
+}
+
 template <typename T>
 __device__ inline T warp_max(T v)
 {
     for (int o = 16; o > 0; o >>= 1)
-    {
-        T w = __shfl_xor_sync(0xffffffffu, v, o);
-        v = v > w ? v : w;
-    }
+        v = nanmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
 
@@ -122,7 +127,7 @@ __device__ inline T block_max(T v, T* sh)
     __syncthreads();
     T r = 0;
     const int nw = (blockDim.x + 31) >> 5;
-    for (int w = 0; w < nw; ++w) r = r > sh[w] ? r : sh[w];
+    for (int w = 0; w < nw; ++w) r = nanmax(r, sh[w]);
     __syncthreads();
     return r;
 }

@@ -8,6 +8,12 @@
 #include "vd_mg.cuh"
 #include "vd_flux.cuh"
 
+// A reference case directory's boundary hooks take three integrated-current
+// arrays more (vidyut_b200/compat defines them); otherwise nothing.
+#ifndef VD_CURRENT_ARGS
+#define VD_CURRENT_ARGS
+#endif
+
 namespace vd {
 
 #define VD_NT (NUM_SPECIES + 1)
@@ -174,7 +180,7 @@ __global__ void k_bc_hook(Geo G, int s, int kind, int comp, double* S, SideArray
             if (user_defined)
                 user_transport::potential_bc(f[0], f[1], f[2], d, sgn, sv, bv, av, bbv, fv,
                                              ga3(G.plo), ga3(G.phi), ga3(G.dx), time, *pp, Tg,
-                                             Pg, app_voltage);
+                                             Pg, app_voltage VD_CURRENT_ARGS);
             else
 #endif
                 plasmachem_transport::potential_bc(f[0], f[1], f[2], d, sgn, sv, bv, av, bbv,
@@ -186,7 +192,7 @@ __global__ void k_bc_hook(Geo G, int s, int kind, int comp, double* S, SideArray
             if (user_defined)
                 user_transport::species_bc(f[0], f[1], f[2], d, sgn, comp, 0, sv, bv, av, bbv,
                                            fv, ga3(G.plo), ga3(G.phi), ga3(G.dx), time, *pp,
-                                           Tg, Pg);
+                                           Tg, Pg VD_CURRENT_ARGS);
             else
 #endif
                 plasmachem_transport::species_bc(f[0], f[1], f[2], d, sgn, comp, 0, sv, bv, av,

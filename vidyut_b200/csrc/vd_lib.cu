@@ -13,6 +13,7 @@
 #include <UserFunctions.H>
 #include <UserSources.H>
 #include <Prob.H>
+#include "vd_probinit.H"
 
 #include "vd_common.cuh"
 #include "vd_kernels.cuh"
@@ -35,6 +36,12 @@ long long g_launches = 0;
 using namespace vd;
 
 namespace {
+using vd::Array4;
+using vd::Box;
+using vd::GeometryData;
+using vd::GpuArray;
+using vd::IntVect;
+using vd::Real;
 
 constexpr int BS = 256;
 
@@ -78,6 +85,7 @@ struct Prof
 {
     int id = VD_PROF_NONE;
     std::vector<cudaEvent_t> a, b;
+    std::vector<int> cnt; // launches inside each timed region
     int n = 0;
     double bytes = 0.0;
     void begin(cudaStream_t st)
@@ -92,9 +100,11 @@ struct Prof
         }
         VD_CUDA_OK(cudaEventRecord(a[n], st));
     }
-    void end(cudaStream_t st)
+    void end(cudaStream_t st, int launches = 1)
     {
         VD_CUDA_OK(cudaEventRecord(b[n], st));
+        if ((int)cnt.size() <= n) cnt.resize(n + 1);
+        cnt[n] = launches;
         ++n;
     }
 };
@@ -284,7 +294,7 @@ void hier_coarsen_coeffs(Hier<T>& H, const int* bct, cudaStream_t st)
             if (bct[s] == MG_ROBIN)
                 LAUNCH(k_mg_robin_coarsen<T>, gsz(plane_count(H.g[l], s % 3)), BS, st,
                        H.g[l - 1], H.g[l], s, H.ra[l - 1][s], H.rb[l - 1][s], H.ra[l][s],
-                       H.rb[l][s], H.c0[l][s], T(H.dx[l][s % 3]));
+                       H.rb[l][s], H.c0[l][s], T(H.dx[l - 1][s % 3]), T(H.dx[l][s % 3]));
     }
 }
 
@@ -344,12 +354,20 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
     if (prof)
         t_prof->bytes = double(3 * sizeof(T)) / 2.0 * (double)op.g.ncell() +
                         (op.b[0] ? double(op.g.dim * sizeof(T)) * (double)op.g.ncell() : 0.0);
+    bool open = false;
+    int timed = 0;
     for (int s = 0; s < n; ++s)
         for (int color = 0; color < 2; ++color)
         {
             const bool fuse = nf && s == 0 && color == 0;
             const bool pf = prof && !fuse; // the timed sweeps are the plain ones
-            if (pf) t_prof->begin(st);
+            // consecutive plain sweeps of one call form one timed region, so
+            // the events do not break the launches' programmatic overlap
+            if (pf && !open)
+            {
+                t_prof->begin(st);
+                open = true;
+            }
             T gamma = op.aconst; // interior diagonal of the constant-coefficient operator
             for (int d = 0; d < op.g.dim; ++d) gamma += op.dh[d] * (op.bconst + op.bconst);
             if (mg3_ok(op))
@@ -434,8 +452,9 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
                            inh ? 1 : 0, T(1) / gamma);
             } else
                 LAUNCH_PDL(k_mg_smooth_color<T>, gsz(half), BS, st, op, x, f, color, inh ? 1 : 0);
-            if (pf) t_prof->end(st);
+            if (pf) ++timed;
         }
+    if (open) t_prof->end(st, timed);
 }
 
 // Launch shape over the cells of a grid: x-blocks along rows, y = j, z = k.
@@ -940,7 +959,7 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
     st.initial_residual = r0;
     st.final_residual = r0;
     st.converged = 1;
-    if (r0 > target)
+    if (!(r0 <= target)) // a NaN residual is not converged
     {
         st.converged = 0;
         const bool refined = cfg.mg_precision == VD_MG_FP32_REFINED && allow32;
@@ -1359,8 +1378,8 @@ void joint_solve(Ctx& c, int first, int nc, double time, const double* Sold,
             const double rq = resid_norm(c, c.HJ[q].op[0], (const double*)c.u[first + q],
                                          (const double*)c.JR[q], (double*)nullptr, true,
                                          bmax ? &bq : nullptr);
-            r = std::max(r, rq);
-            b = std::max(b, bq);
+            r = nanmax(r, rq);
+            b = nanmax(b, bq);
         }
         if (bmax) *bmax = b;
         return r;
@@ -1601,9 +1620,9 @@ __global__ void k_initdomain(Geo G, double* S, const ProbParm* pp)
     {
         int i, j, k;
         cell_of(G.g, t, i, j, k);
-        Array4 v = state_view(S, G.g);
+        vd::Array4 v = state_view(S, G.g);
         v.clamp = 0;
-        GeometryData gd;
+        vd::GeometryData gd;
         for (int d = 0; d < 3; ++d)
         {
             gd.prob_lo[d] = G.plo[d];
@@ -1611,8 +1630,9 @@ __global__ void k_initdomain(Geo G, double* S, const ProbParm* pp)
             gd.dx[d] = G.dx[d];
             gd.n_cell[d] = G.g.n[d];
         }
-        Box bx{{i, j, k}, {i, j, k}};
-        initdomaindata(bx, v, gd, pp);
+        vd::Box bx{{i, j, k}, {i, j, k}};
+        // a reference Prob.H takes a non-const ProbParm* (it only reads it)
+        initdomaindata(bx, v, gd, const_cast<ProbParm*>(pp));
     }
 }
 
@@ -2312,10 +2332,8 @@ vd_status vd_destroy(void* ctx)
 vd_status vd_init_domain(void* ctx, const char* prob_inputs)
 {
     VD_TRY({
-        auto table = vd::ParmParse::parse(prob_inputs ? prob_inputs : "");
-        vd::ParmParse pp(&table, "prob");
         c->hpp = ProbParm{};
-        amrex_probinit(c->hpp, pp);
+        vd_probinit(c->hpp, prob_inputs);
         VD_CUDA_OK(cudaMemcpyAsync(c->dpp, &c->hpp, sizeof(ProbParm), cudaMemcpyHostToDevice, c->st));
         LAUNCH(k_initdomain, gsz(c->N), BS, c->st, c->G, c->S, c->dpp);
         c->time = 0.0;
@@ -2432,23 +2450,26 @@ vd_status vd_profile_read(void* ctx, long long* launches, double* total_ms,
     long long used = 0;
     VD_TRY({
         std::vector<float> t(c->prof.n);
+        std::vector<float> per(c->prof.n);
         for (int i = 0; i < c->prof.n; ++i)
         {
             VD_CUDA_OK(cudaEventSynchronize(c->prof.b[i]));
             VD_CUDA_OK(cudaEventElapsedTime(&t[i], c->prof.a[i], c->prof.b[i]));
+            per[i] = t[i] / (c->prof.cnt[i] > 0 ? c->prof.cnt[i] : 1);
         }
         // V-cycles are enqueued in batches, and the launches of a cycle
         // enqueued past convergence return at once on the stop flag (a few
         // µs against tens for a working sweep): those did no work and are
-        // left out, by duration, below a quarter of the median launch
-        std::vector<float> srt = t;
+        // left out, by their per-launch duration, below a quarter of the
+        // median
+        std::vector<float> srt = per;
         std::sort(srt.begin(), srt.end());
         const float cut = srt.empty() ? 0.f : 0.25f * srt[srt.size() / 2];
-        for (float ms : t)
-            if (ms >= cut)
+        for (int i = 0; i < c->prof.n; ++i)
+            if (per[i] >= cut)
             {
-                tot += ms;
-                ++used;
+                tot += t[i];
+                used += c->prof.cnt[i] > 0 ? c->prof.cnt[i] : 1;
             }
     });
     if (launches) *launches = used;
@@ -2643,6 +2664,12 @@ vd_status vd_last_error(void* ctx, char* buf, int len)
 // process exits.
 // ======================================================================
 namespace {
+using vd::Array4;
+using vd::Box;
+using vd::GeometryData;
+using vd::GpuArray;
+using vd::IntVect;
+using vd::Real;
 
 constexpr long long VD_NA_SCRATCH_DOUBLES = 1LL << 20; // 8 MiB per device
 constexpr int VD_NA_MAX_LEVELS = 16;

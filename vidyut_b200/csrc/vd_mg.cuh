@@ -886,7 +886,7 @@ __global__ void __launch_bounds__(256, VARB ? VD_SWEEP_VARB_MINB : (NORM ? VD_SW
                                                             j, k, inhomog != 0));
                 const double rb = fabs((double)mg3_residual(L, vf[u].y, v0[u].y, rB, bB, oB, iB,
                                                             j, k, inhomog != 0));
-                mres = fmax(mres, fmax(ra, rb));
+                mres = nanmax(mres, nanmax(ra, rb));
             }
             V2 o;
             o.x = mg3_gs_value<T, VARB>(L, iA, j, k, oA, inhomog != 0, inv_gamma, vf[u].x, nA);
@@ -929,7 +929,7 @@ __global__ void __launch_bounds__(256, VARB ? VD_SWEEP_VARB_MINB : (NORM ? VD_SW
 #pragma unroll
                 for (int m = 0; m < 6; ++m) rn[m] = nb[m];
                 mg3_faces<T, VARB>(L, i, j, k, b);
-                mres = fmax(mres, fabs((double)mg3_residual(L, fv, __ldg(xs + h), rn, b, out, i,
+                mres = nanmax(mres, fabs((double)mg3_residual(L, fv, __ldg(xs + h), rn, b, out, i,
                                                             j, k, inhomog != 0)));
             }
             const T v = mg3_gs_value<T, VARB>(L, i, j, k, out, inhomog != 0, inv_gamma, fv, nb);
@@ -1173,11 +1173,11 @@ __global__ void __launch_bounds__(256, 4) k_mg_resid3v(const __grid_constant__ M
             x32[o] = 0.0f;
         }
         const double a = fabs((double)r);
-        m = a > m ? a : m;
+        m = nanmax(m, a);
         if (fnorm)
         {
             const double af = fabs((double)fv);
-            mf = af > mf ? af : mf;
+            mf = nanmax(mf, af);
         }
     };
     for (int col = 0; col < (both ? 2 : 1); ++col)
@@ -1367,11 +1367,11 @@ __global__ void __launch_bounds__(256, 4) k_mg_resid3(const __grid_constant__ MG
                     x32[col * half + hb + u * plane] = 0.0f;
                 }
                 const double a = fabs((double)r);
-                m = a > m ? a : m;
+                m = nanmax(m, a);
                 if (fnorm)
                 {
                     const double af = fabs((double)v[u][7]);
-                    mf = af > mf ? af : mf;
+                    mf = nanmax(mf, af);
                 }
             }
             continue;
@@ -1412,11 +1412,11 @@ __global__ void __launch_bounds__(256, 4) k_mg_resid3(const __grid_constant__ MG
                 x32[o] = 0.0f;
             }
             const double a = fabs((double)r);
-            m = a > m ? a : m;
+            m = nanmax(m, a);
             if (fnorm)
             {
                 const double af = fabs((double)v[u][7]);
-                mf = af > mf ? af : mf;
+                mf = nanmax(mf, af);
             }
         }
     }
@@ -1545,11 +1545,11 @@ __global__ void __launch_bounds__(128) k_mg_resid_norm(MGOp<T> L, const T* __res
             const T rr = f[p] - mg_apply_any(L, x, i, j, k, inhomog != 0);
             if (rout) rout[p] = rr;
             const double a = fabs((double)rr);
-            m = a > m ? a : m;
+            m = nanmax(m, a);
             if (fnorm)
             {
                 const double af = fabs((double)f[p]);
-                mf = af > mf ? af : mf;
+                mf = nanmax(mf, af);
             }
         }
     m = block_max(m, sh);
@@ -1602,11 +1602,11 @@ __global__ void __launch_bounds__(256) k_mg_resid_norm_rb(MGOp<T> L, const T* __
             const T rr = f[p] - mg_apply_any(L, x, i, j, k, inhomog != 0);
             if (rout) rout[p] = rr;
             const double a = fabs((double)rr);
-            m = a > m ? a : m;
+            m = nanmax(m, a);
             if (fnorm)
             {
                 const double af = fabs((double)f[p]);
-                mf = af > mf ? af : mf;
+                mf = nanmax(mf, af);
             }
         }
     }
@@ -1632,8 +1632,8 @@ __global__ void __launch_bounds__(1024) k_mg_max_partials(MGOp<T> L, const doubl
     double m = 0.0, mf = 0.0;
     for (long long b = threadIdx.x; b < nb; b += blockDim.x)
     {
-        m = part[b] > m ? part[b] : m;
-        if (fnorm) mf = part[nb + b] > mf ? part[nb + b] : mf;
+        m = nanmax(m, part[b]);
+        if (fnorm) mf = nanmax(mf, part[nb + b]);
     }
     m = block_max(m, sh);
     if (fnorm) mf = block_max(mf, sh);
@@ -1686,7 +1686,7 @@ __device__ void mg_bottom_block(const MGOp<T>& L, T* __restrict__ x, const T* __
         p[q] = T(0);
         v[q] = T(0);
         const T a = r[q] < T(0) ? -r[q] : r[q];
-        m = a > m ? a : m;
+        m = nanmax(m, a);
     }
     const T rnorm0 = block_max(m, sh);
     int ret = 0;
@@ -1735,7 +1735,7 @@ __device__ void mg_bottom_block(const MGOp<T>& L, T* __restrict__ x, const T* __
                 x[q] += alpha * p[q];
                 s[q] = r[q] - alpha * v[q];
                 const T a = s[q] < T(0) ? -s[q] : s[q];
-                m = a > m ? a : m;
+                m = nanmax(m, a);
             }
             if (block_max(m, sh) <= rel * rnorm0)
             {
@@ -1765,7 +1765,7 @@ __device__ void mg_bottom_block(const MGOp<T>& L, T* __restrict__ x, const T* __
                 x[q] += omega * s[q];
                 r[q] = s[q] - omega * tt[q];
                 const T a = r[q] < T(0) ? -r[q] : r[q];
-                m = a > m ? a : m;
+                m = nanmax(m, a);
             }
             if (block_max(m, sh) <= rel * rnorm0)
             {
@@ -2552,11 +2552,27 @@ __global__ void k_mg_avg_faces(GridDev gf, GridDev gc, int d, const T* __restric
     }
 }
 
-// Robin coefficients on a coarse boundary side: mean of the fine a,b over
-// the 2^(dim-1) fine faces, then c0 = (b/dx - a/2) / (a/2 + b/dx).
+// Robin coefficients on a coarse boundary side.  A face a*phi + b*dphi/dn = f
+// closed by the two-point ghost over a cell of width h passes the
+// homogeneous flux -kappa*phi_inside, kappa = a / (a h/2 + b) (2/h for
+// Dirichlet, 0 for Neumann).  The coarse face keeps the mean conductance of
+// its 2^(dim-1) fine faces (width dxf), capped at its own Dirichlet value
+// 2/dxc, as the Dirichlet weight w = min(1, mean(kappa) dxc/2) stored as
+// (a, b) = (w, (1 - w) dxc/2): uniform Dirichlet and Neumann sides coarsen
+// to themselves exactly, a uniform weak Robin side keeps its conductance,
+// and Dirichlet patches in a Neumann wall keep their share of the flux
+// (averaging a and b apart turns such a wall nearly Neumann on the coarse
+// levels and the V-cycle diverges); then c0 = (b/dx - a/2) / (a/2 + b/dx).
+template <typename T>
+__device__ __forceinline__ T robin_conductance(T a, T b, T h)
+{
+    const T den = T(0.5) * a * h + b;
+    return den != T(0) ? a / den : T(0);
+}
+
 template <typename T>
 __global__ void k_mg_robin_coarsen(GridDev gf, GridDev gc, int s, const T* ra_f,
-                                   const T* rb_f, T* ra_c, T* rb_c, T* c0_c, T dxc)
+                                   const T* rb_f, T* ra_c, T* rb_c, T* c0_c, T dxf, T dxc)
 {
     VD_PDL_WAIT();
     const int d = s % 3;
@@ -2567,7 +2583,7 @@ __global__ void k_mg_robin_coarsen(GridDev gf, GridDev gc, int s, const T* ra_f,
          q += gridDim.x * blockDim.x)
     {
         const int ia = q % na, ib = q / na;
-        T sa = T(0), sb = T(0);
+        T sk = T(0);
         int cnt = 0;
         for (int u = 0; u < 2; ++u)
             for (int w = 0; w < (tb_active ? 2 : 1); ++w)
@@ -2575,11 +2591,11 @@ __global__ void k_mg_robin_coarsen(GridDev gf, GridDev gc, int s, const T* ra_f,
                 const int fa = 2 * ia + u;
                 const int fb = tb_active ? 2 * ib + w : ib;
                 const int fp = fa + gf.n[ta] * fb;
-                sa += ra_f[fp];
-                sb += rb_f[fp];
+                sk += robin_conductance(ra_f[fp], rb_f[fp], dxf);
                 ++cnt;
             }
-        const T a = sa / T(cnt), b = sb / T(cnt);
+        const T kd = (sk / T(cnt)) * (T(0.5) * dxc);
+        const T a = kd < T(1) ? kd : T(1), b = (T(1) - a) * (T(0.5) * dxc);
         ra_c[q] = a;
         rb_c[q] = b;
         const T dxi = T(1) / dxc;
