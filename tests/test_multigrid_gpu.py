@@ -9,6 +9,7 @@ py_utils/compare_fields_from_twoplotfiles.py:40-46) with V-cycle counts
 within one of each other."""
 import ctypes
 
+import numpy as np
 import pytest
 
 import vidyut_b200 as vb
@@ -187,3 +188,29 @@ def test_poisson_stops_at_maxiter(require_gpu, maxiter):
     assert abs(sg.final_residual - so.final_residual) <= 1e-9 * so.final_residual
     pid = g.info["pot_id"]
     assert rel(g.get_state(pid, 1), o.get_state(pid, 1)) < 1e-12
+
+
+# The TMA-staged sweeps (vd_mg_tma.cuh) against the register-staged ones on
+# the same levels (threshold lowered to one cell, as above): the same cell
+# arithmetic on the same neighbour values, so the same V-cycle count and the
+# same bits.  Shapes with partial tiles in x (nx/2 < 64, not a multiple of
+# 64) and y (ny not a multiple of 16), two tiles across x, odd plane counts
+# per CTA; FP64 and the FP32-refined form (FP32 levels whose half-row is not
+# a multiple of 16 bytes keep the register-staged sweep).
+@pytest.mark.parametrize("shape", [(64, 64, 48), (72, 40, 36), (256, 32, 16), (96, 64, 70)])
+@pytest.mark.parametrize("precision", [vb.VD_MG_FP64, vb.VD_MG_FP32_REFINED])
+def test_tma_sweeps_equal_register_sweeps(require_gpu, monkeypatch, shape, precision):
+    monkeypatch.setenv("VD_MG_BIG_LEVEL_CELLS", "1")
+    runs = []
+    for tma in ("1", "0"):
+        monkeypatch.setenv("VD_MG_TMA", tma)
+        cfg = box(*shape, mg_precision=precision)
+        if precision == vb.VD_MG_FP32_REFINED:
+            cfg["linsolve_reltol"] = 1e-10
+        g = vb.Vidyut(cfg)
+        g.set_state(0, W.initial_state(cfg, 31))
+        st = g.solve_potential(0.0)
+        runs.append((st.iterations, st.final_residual, g.get_state(g.info["pot_id"], 1)))
+        g.close()
+    assert runs[0][0] == runs[1][0] and runs[0][1] == runs[1][1]
+    assert np.array_equal(runs[0][2], runs[1][2])

@@ -17,6 +17,7 @@
 
 #include "vd_common.cuh"
 #include "vd_kernels.cuh"
+#include "vd_mg_tma.cuh"
 #include "vd_adjoint.cuh"
 
 #include <algorithm>
@@ -241,17 +242,29 @@ static long long big_level_cells()
     return v > 0 ? v : (8LL << 20);
 }
 
+// TMA-staged sweeps on the big constant-coefficient levels when the
+// environment variable VD_MG_TMA is 1 (the register-staged sweeps are
+// faster on B200 and stay the default; the two give the same bits, and
+// tests compare them).
+static int tma_sweeps()
+{
+    const char* e = std::getenv("VD_MG_TMA");
+    return (e && e[0] == '1') ? 1 : 0;
+}
+
 template <typename T>
 void hier_set_ops(Hier<T>& H, double aconst, double beta, double bconst, const int* bct,
                   int maxorder)
 {
     H.op.assign(H.nlev, MGOp<T>{});
     const long long big = big_level_cells();
+    const int tma = tma_sweeps();
     for (int l = 0; l < H.nlev; ++l)
     {
         MGOp<T>& o = H.op[l];
         o.g = H.g[l];
         o.big_cells = big;
+        o.tma = tma;
         for (int d = 0; d < 3; ++d)
             o.dh[d] = (d < H.dim) ? T(beta / (H.dx[l][d] * H.dx[l][d])) : T(0);
         o.aconst = T(aconst);
@@ -338,6 +351,95 @@ bool norm_fusable(const MGOp<T>& op, long long npart)
     return nb <= npart;
 }
 
+// cuTensorMapEncodeTiled from the driver, through the runtime's entry-point
+// query (no link against libcuda); null if the driver does not offer it.
+using TmaEncodeFn = decltype(&cuTensorMapEncodeTiled);
+static TmaEncodeFn tma_encode_fn()
+{
+    static const TmaEncodeFn fn = []() -> TmaEncodeFn {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<TmaEncodeFn>(p);
+    }();
+    return fn;
+}
+
+// Tensor map of one colour half of a 3-D split level: dims (nxh, ny, nz),
+// box (bx, by, 1), zero fill outside.  False where TMA cannot address it
+// (base or row pitch not a multiple of 16 bytes).
+template <typename T>
+static bool tma_map_half(CUtensorMap* m, const T* base, const GridDev& g, int bx, int by)
+{
+    const TmaEncodeFn enc = tma_encode_fn();
+    const long long nxh = g.n[0] / 2;
+    if (!enc || (reinterpret_cast<uintptr_t>(base) & 15) || (nxh * (long long)sizeof(T)) % 16)
+        return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)nxh, (cuuint64_t)g.n[1], (cuuint64_t)g.n[2]};
+    const cuuint64_t strides[2] = {(cuuint64_t)(nxh * sizeof(T)),
+                                   (cuuint64_t)(nxh * g.n[1] * sizeof(T))};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return enc(m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+               3, const_cast<T*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+static int sm_count()
+{
+    static int n[64] = {};
+    int dev = 0;
+    VD_CUDA_OK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!n[dev]) VD_CUDA_OK(cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev));
+    return n[dev];
+}
+
+// Launch shape of a TMA-staged sweep: the level's tiles times the z-chunks
+// that fill two CTAs per SM (at least one chunk; nzc chunks of a plane each
+// at most).  Returns the grid size; *nzc gets the chunk count.
+template <typename T>
+static int tma_sweep_grid(const GridDev& g, int* nzc = nullptr)
+{
+    using S = TmaSweepShape<T, false>;
+    const int ntiles = ((g.n[0] / 2 + TMA_TX - 1) / TMA_TX) * ((g.n[1] + S::TY - 1) / S::TY);
+    const int chunks = std::max(1, std::min(g.n[2], S::MINB * sm_count() / ntiles));
+    if (nzc) *nzc = chunks;
+    return ntiles * chunks;
+}
+
+// One colour sweep of a big constant-coefficient level with TMA-staged
+// operands; false (nothing launched) where the level cannot take it.
+template <typename T, bool PROL, bool NORM>
+static bool sweep_tma(const MGOp<T>& op, T* x, const T* f, int color, bool inh, T ig,
+                      const GridDev& gcv, const T* xc, double* part, cudaStream_t st)
+{
+    using S = TmaSweepShape<T, NORM>;
+    const long long half = op.g.ncell() / 2;
+    CUtensorMap mx, mf, mv;
+    if (!tma_map_half(&mx, x + (1 - color) * half, op.g, TMA_TX + 2 * S::XH, S::TY + 2) ||
+        !tma_map_half(&mf, f + color * half, op.g, TMA_TX, S::TY))
+        return false;
+    if (NORM && !tma_map_half(&mv, x + color * half, op.g, TMA_TX, S::TY)) return false;
+    if (!NORM) mv = mf;
+    static bool attr = false;
+    if (!attr)
+    {
+        VD_CUDA_OK(cudaFuncSetAttribute(k_mg_sweep3t<T, PROL, NORM>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
+        attr = true;
+    }
+    int nzc = 1;
+    const int grid = tma_sweep_grid<T>(op.g, &nzc);
+    launch_pdl(k_mg_sweep3t<T, PROL, NORM>, dim3(grid), dim3(S::THREADS), (size_t)S::SMEM, st, op,
+               mx, mf, mv, x, color, inh ? 1 : 0, ig, gcv, xc, part, op.err, nzc);
+    return true;
+}
+
 // n Gauss-Seidel iterations (colour 0, colour 1).  With xc given (only for
 // mg3_ok levels) the first colour-0 sweep also adds the prolongated coarse
 // correction xc of level gc; with nf given (norm_fusable levels) it also
@@ -389,16 +491,27 @@ void smooth(const MGOp<T>& op, T* x, const T* f, bool inh, int n, cudaStream_t s
 #define VD_SWEEP3N(VB, UV)                                                                    \
     LAUNCH_PDL((k_mg_sweep3v<T, VB, false, UV, true>), gv, 256, st, op, x, f, color,          \
                inh ? 1 : 0, ig, gcv, xc, nf->part)
+                    // big constant-coefficient levels: TMA-staged sweeps
+                    const bool tma = two && op.tma && op.err && !op.b[0];
                     if (fuse)
                     {
-                        if (op.b[0])
+                        long long nbv = (long long)gv.x * gv.y * gv.z;
+                        if (tma && sweep_tma<T, false, true>(op, x, f, color, inh, ig, gcv, xc,
+                                                             nf->part, st))
+                            nbv = tma_sweep_grid<T>(op.g);
+                        else if (op.b[0])
                             { if (two) VD_SWEEP3N(true, 2); else VD_SWEEP3N(true, 1); }
                         else
                             { if (two) VD_SWEEP3N(false, 2); else VD_SWEEP3N(false, 1); }
-                        const long long nbv = (long long)gv.x * gv.y * gv.z;
                         LAUNCH_PDL(k_mg_max_partials<T>, 1, 1024, st, op, nf->part, nbv, 0,
                                    &nf->dmg->rbits);
                         LAUNCH_PDL(k_mg_check, 1, 1, st, nf->dmg, nf->target);
+                    } else if (tma && (pro ? sweep_tma<T, true, false>(op, x, f, color, inh, ig, gcv,
+                                                                       xc, nullptr, st)
+                                           : sweep_tma<T, false, false>(op, x, f, color, inh, ig,
+                                                                        gcv, xc, nullptr, st)))
+                    {
+                        // launched
                     } else if (op.b[0] && pro)
                         { if (two) VD_SWEEP3V(true, true, 2); else VD_SWEEP3V(true, true, 1); }
                     else if (op.b[0])
@@ -977,7 +1090,11 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
             VD_CUDA_OK(cudaMemcpyAsync(c.dmg, &init, sizeof(MGDev), cudaMemcpyHostToDevice, c.st));
             MGOp<double> op0 = H64.op[0];
             op0.stop = &c.dmg->done;
-            for (auto& o : H32.op) o.stop = &c.dmg->done;
+            for (auto& o : H32.op)
+            {
+                o.stop = &c.dmg->done;
+                o.err = &c.dmg->tma_err;
+            }
             int issued = 0;
             int batch = std::max(1, (hint + inner - 1) / inner - 1);
             while (issued * inner < cfg.linsolve_maxiter)
@@ -1009,7 +1126,8 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
                 VD_CUDA_OK(cudaMemcpyAsync(c.hmg, c.dmg, sizeof(MGDev), cudaMemcpyDeviceToHost, c.st));
                 VD_CUDA_OK(cudaStreamSynchronize(c.st));
             }
-            for (auto& o : H32.op) o.stop = nullptr;
+            for (auto& o : H32.op) o.stop = nullptr, o.err = nullptr;
+            if (c.hmg->tma_err) throw CudaError("a TMA-staged multigrid sweep timed out");
             st.iterations = c.hmg->iters;
             st.refinements = c.hmg->refs;
             std::memcpy(&st.final_residual, &c.hmg->final_bits, sizeof(double));
@@ -1047,7 +1165,11 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
             // when the device-side stop flag is up, so the iteration count
             // and result equal those of a cycle-by-cycle host loop
             VD_CUDA_OK(cudaMemsetAsync(c.dmg, 0, sizeof(MGDev), c.st));
-            for (auto& o : H64.op) o.stop = &c.dmg->done;
+            for (auto& o : H64.op)
+            {
+                o.stop = &c.dmg->done;
+                o.err = &c.dmg->tma_err;
+            }
             MGOp<double> op0 = H64.op[0];
             // the norm of cycle v's result is taken by the first sweep of
             // cycle v+1 (NormFuse): the check lags one cycle, and a converged
@@ -1088,7 +1210,8 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
                 VD_CUDA_OK(cudaMemcpyAsync(c.hmg, c.dmg, sizeof(MGDev), cudaMemcpyDeviceToHost, c.st));
                 VD_CUDA_OK(cudaStreamSynchronize(c.st));
             }
-            for (auto& o : H64.op) o.stop = nullptr;
+            for (auto& o : H64.op) o.stop = nullptr, o.err = nullptr;
+            if (c.hmg->tma_err) throw CudaError("a TMA-staged multigrid sweep timed out");
             st.iterations = c.hmg->iters;
             std::memcpy(&st.final_residual, &c.hmg->final_bits, sizeof(double));
             st.converged = c.hmg->done;

@@ -49,8 +49,10 @@ struct MGOp
     const T* c0[6];
     const T* gv[6];
     const int* stop; // set to non-zero on the device once the solve has converged
+    int* err;        // device word a TMA-staged sweep sets when a wait gives up
     long long big_cells; // host only: levels of at least this many cells (0: 8 M) take the
                          // sweeps built for HBM-resident levels
+    int tma;             // host only: those levels' constant-coefficient sweeps are TMA-staged
 };
 
 template <typename T>
@@ -2635,6 +2637,7 @@ struct MGDev
     int refs;       // refinement passes of the FP32-refined form
     double sc_cur;  // scale of the FP32 right-hand side being solved for
     double sc_next; // 1 / max-norm of the latest residual
+    int tma_err;    // a TMA-staged sweep gave up waiting for its copies
 };
 
 // After each V-cycle: count it and raise the stop flag once the residual
