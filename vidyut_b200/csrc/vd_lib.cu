@@ -1093,7 +1093,7 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
             for (auto& o : H32.op)
             {
                 o.stop = &c.dmg->done;
-                o.err = &c.dmg->tma_err;
+                o.err = &c.dmg->wait_err;
             }
             int issued = 0;
             int batch = std::max(1, (hint + inner - 1) / inner - 1);
@@ -1127,7 +1127,7 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
                 VD_CUDA_OK(cudaStreamSynchronize(c.st));
             }
             for (auto& o : H32.op) o.stop = nullptr, o.err = nullptr;
-            if (c.hmg->tma_err) throw CudaError("a TMA-staged multigrid sweep timed out");
+            if (c.hmg->wait_err) throw CudaError("a multigrid kernel's bounded wait gave up");
             st.iterations = c.hmg->iters;
             st.refinements = c.hmg->refs;
             std::memcpy(&st.final_residual, &c.hmg->final_bits, sizeof(double));
@@ -1168,7 +1168,7 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
             for (auto& o : H64.op)
             {
                 o.stop = &c.dmg->done;
-                o.err = &c.dmg->tma_err;
+                o.err = &c.dmg->wait_err;
             }
             MGOp<double> op0 = H64.op[0];
             // the norm of cycle v's result is taken by the first sweep of
@@ -1211,7 +1211,7 @@ int mg_solve(Ctx& c, Hier<double>& H64, Hier<float>& H32, double* sol, double* r
                 VD_CUDA_OK(cudaStreamSynchronize(c.st));
             }
             for (auto& o : H64.op) o.stop = nullptr, o.err = nullptr;
-            if (c.hmg->tma_err) throw CudaError("a TMA-staged multigrid sweep timed out");
+            if (c.hmg->wait_err) throw CudaError("a multigrid kernel's bounded wait gave up");
             st.iterations = c.hmg->iters;
             std::memcpy(&st.final_residual, &c.hmg->final_bits, sizeof(double));
             st.converged = c.hmg->done;

@@ -2637,7 +2637,7 @@ struct MGDev
     int refs;       // refinement passes of the FP32-refined form
     double sc_cur;  // scale of the FP32 right-hand side being solved for
     double sc_next; // 1 / max-norm of the latest residual
-    int tma_err;    // a TMA-staged sweep gave up waiting for its copies
+    int wait_err;   // a TMA-staged sweep gave up waiting for its copies
 };
 
 // After each V-cycle: count it and raise the stop flag once the residual
