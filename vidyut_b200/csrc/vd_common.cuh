@@ -36,6 +36,12 @@ struct UnsupportedError : CudaError
     explicit UnsupportedError(std::string m) : CudaError(std::move(m)) {}
 };
 
+// A device allocation that failed for lack of memory (VD_ERR_OOM).
+struct OomError : CudaError
+{
+    explicit OomError(std::string m) : CudaError(std::move(m)) {}
+};
+
 // Grid of one multigrid level (or of the state): cell counts, active
 // dimension count, periodicity, storage layout.
 //   natural (rb = 0): (i,j,k) -> i + nx*(j + ny*k)            (the state)

@@ -111,16 +111,38 @@ struct Prof
 };
 thread_local Prof* t_prof = nullptr;
 
+// Allocations left before a simulated out-of-memory failure (host-side
+// fault injection for tests: VD_FAULT_ALLOC_AFTER=n makes the allocation
+// after the n-th of a context fail as cudaMalloc does when the device is
+// full); -1: off.
+static long long fault_alloc_after()
+{
+    const char* e = std::getenv("VD_FAULT_ALLOC_AFTER");
+    return (e && *e) ? std::atoll(e) : -1;
+}
+
 struct Alloc
 {
     std::vector<void*> ptrs;
+    long long fault_after = fault_alloc_after();
     template <class T>
     T* get(size_t n)
     {
         if (n == 0) n = 1;
         void* p = nullptr;
-        if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess)
-            throw CudaError("cudaMalloc of " + std::to_string(n * sizeof(T)) + " bytes failed");
+        const size_t bytes = n * sizeof(T);
+        if (fault_after >= 0 && (long long)ptrs.size() >= fault_after)
+            throw OomError("cudaMalloc of " + std::to_string(bytes) +
+                           " bytes failed: out of memory (injected by VD_FAULT_ALLOC_AFTER)");
+        const cudaError_t r = cudaMalloc(&p, bytes);
+        if (r == cudaErrorMemoryAllocation)
+        {
+            cudaGetLastError(); // not sticky: clear it for the calls that follow
+            throw OomError("cudaMalloc of " + std::to_string(bytes) + " bytes failed: out of memory");
+        }
+        if (r != cudaSuccess)
+            throw CudaError("cudaMalloc of " + std::to_string(bytes) + " bytes failed: " +
+                            cudaGetErrorString(r));
         ptrs.push_back(p);
         return static_cast<T*>(p);
     }
@@ -2402,11 +2424,10 @@ vd_status vd_create(const vd_config* cfg, void** out)
     } catch (const CudaError& e)
     {
         const bool unsup = dynamic_cast<const UnsupportedError*>(&e) != nullptr;
+        const bool oom = dynamic_cast<const OomError*>(&e) != nullptr;
         g_create_err = e.msg;
-        c->A.release();
-        if (c->hcoarse) cudaFreeHost(c->hcoarse);
-        delete c;
-        return unsup ? VD_ERR_UNSUPPORTED : VD_ERR_CUDA;
+        vd_destroy(c); // everything made so far: device and pinned memory, stream, events
+        return unsup ? VD_ERR_UNSUPPORTED : (oom ? VD_ERR_OOM : VD_ERR_CUDA);
     }
     *out = c;
     return VD_OK;
@@ -2446,6 +2467,10 @@ vd_status vd_destroy(void* ctx)
     {                                                                            \
         c->err = e.msg;                                                          \
         return VD_ERR_UNSUPPORTED;                                               \
+    } catch (const OomError& e)                                                  \
+    {                                                                            \
+        c->err = e.msg;                                                          \
+        return VD_ERR_OOM;                                                       \
     } catch (const CudaError& e)                                                 \
     {                                                                            \
         c->err = e.msg;                                                          \
