@@ -81,7 +81,7 @@ VD_HD inline Dim3 lbound(const Box& b) { return {b.lo[0], b.lo[1], b.lo[2]}; }
 VD_HD inline Dim3 ubound(const Box& b) { return {b.hi[0], b.hi[1], b.hi[2]}; }
 
 // ParmParse over the parameter table the library hands to amrex_probinit
-// (set for the duration of that call, see VD_PROBINIT in vd_lib.cu).
+// (set for the duration of that call by vd_probinit, vd_probinit.H).
 class ParmParse
 {
 public:
