@@ -1141,7 +1141,17 @@ __global__ void __launch_bounds__(256, VD_RESTRICT_MINB) k_mg_restrict3(const __
 // 16-byte accesses (nx % 4 == 0), as k_mg_sweep3v; outputs and arguments as
 // k_mg_resid3.  Blocks of 32 pairs by 8 rows, MG3_U planes per thread.
 template <typename T, bool VARB>
-__global__ void __launch_bounds__(256, 4) k_mg_resid3v(const __grid_constant__ MGOp<T> L,
+// CTAs per SM the residual's registers are sized for: 3 (80 registers) for
+// constant coefficients and 2 (128) for face coefficients; at 4 (64) both
+// spilled 112-240 B (measured at 256^3: 18.78-18.82 -> 18.68 ms per step).
+#ifndef VD_RESID_MINB
+#define VD_RESID_MINB 3
+#endif
+#ifndef VD_RESID_VARB_MINB
+#define VD_RESID_VARB_MINB 2
+#endif
+__global__ void __launch_bounds__(256, VARB ? VD_RESID_VARB_MINB : VD_RESID_MINB)
+    k_mg_resid3v(const __grid_constant__ MGOp<T> L,
                                                        const T* __restrict__ x,
                                                        const T* __restrict__ f,
                                                        T* __restrict__ rout, int inhomog,
