@@ -214,3 +214,47 @@ def test_tma_sweeps_equal_register_sweeps(require_gpu, monkeypatch, shape, preci
         g.close()
     assert runs[0][0] == runs[1][0] and runs[0][1] == runs[1][1]
     assert np.array_equal(runs[0][2], runs[1][2])
+
+
+# Species face coefficients in one pass per species (k_species_faces3: each
+# cell's diffusivity evaluated once) against one launch per direction
+# (VD_SPECIES_FACES3=0): the same values and harmonic means, so the same
+# solve bit for bit; periodic and walled sides, 3-D and 2-D, and the LMEA
+# mechanism, whose diffusivities read the state.
+@pytest.mark.parametrize("kind", ["box", "periodic", "2d", "lmea"])
+def test_species_faces_one_pass_equal_per_direction(require_gpu, monkeypatch, kind):
+    def make():
+        if kind == "lmea":
+            cfg = W.lmea_config(24)
+            return cfg, W.lmea_state(cfg, 3)
+        if kind == "2d":
+            cfg = W.townsend_config(2, 64)
+            return cfg, W.initial_state(cfg, 3)
+        cfg = box(64, 40, 36) if kind == "box" else box(
+            64, 40, 36, pot_lo=(0, 0, 1), pot_hi=(0, 0, 1))
+        if kind == "periodic":
+            cfg["is_periodic"] = [1, 1, 0]
+            for key in ("eden", "ion", "neutral", "eenrg"):
+                cfg[f"{key}_bc_lo"] = [0, 0, 2]
+                cfg[f"{key}_bc_hi"] = [0, 0, 2]
+        return cfg, W.initial_state(cfg, 3)
+
+    runs = []
+    for v in ("1", "0"):
+        monkeypatch.setenv("VD_SPECIES_FACES3", v)
+        cfg, S = make()
+        g = vb.Vidyut(cfg)
+        g.set_state(0, S)
+        g.solve_potential(0.0, allow_unconverged=True)
+        ex = g.explicit_rhs(0.0)
+        out = []
+        for spec in range(2):
+            g.set_state(0, S)
+            st = g.implicit_solve_scalar(spec, ex, 0.0, allow_unconverged=True)
+            out.append((st.iterations, g.get_state(spec, 1)))
+        g.step(2, allow_unconverged=True)
+        out.append((0, g.get_state()))
+        g.close()
+        runs.append(out)
+    for a, b in zip(*runs):
+        assert a[0] == b[0] and np.array_equal(a[1], b[1])

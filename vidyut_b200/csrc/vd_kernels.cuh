@@ -896,6 +896,73 @@ __global__ void k_species_faces(GridDev g, int d, const double* __restrict__ S, 
     }
 }
 
+// The same face coefficients for every direction in one pass, each cell's
+// diffusivity evaluated once (k_species_faces evaluates it at both cells of
+// every face, once per direction: six times per cell, each with the state
+// loads the hook needs).  A 32 x 8 block of cells marches over a chunk of
+// planes; a plane's diffusivities go to shared memory with a one-cell halo
+// on the low x and y sides (the lower neighbours of the block's first
+// column and row), the previous plane's stays in a register for the z
+// faces, and the faces past the last cell of a row, column or plane take
+// the neighbour as cell_diff clamps (or wraps) it.  Same values and the same
+// harmonic mean as k_species_faces, so the same bits.
+__global__ void __launch_bounds__(256) k_species_faces3(GridDev g, const double* __restrict__ S,
+                                                        int spec, double Tg, int kchunk,
+                                                        double* __restrict__ bx,
+                                                        double* __restrict__ by,
+                                                        double* __restrict__ bz)
+{
+    VD_PDL_WAIT();
+    __shared__ double sd[8][33]; // column 0: the halo i0-1, columns 1..32 the block
+    __shared__ double sy[32];    // the halo row j0-1
+    const long long N = g.ncell();
+    const int nx = g.n[0], ny = g.n[1], nz = g.n[2], dim = g.dim;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int i = blockIdx.x * 32 + tx, j = blockIdx.y * 8 + ty;
+    const bool act = i < nx && j < ny;
+    const int kb = blockIdx.z * kchunk, ke = min(nz, kb + kchunk);
+    auto hm = [](double d0, double d1) {
+        const double den = d0 + d1;
+        return (den != 0.0) ? 2.0 * d0 * d1 / den : 0.0;
+    };
+    double dprev = 0.0;
+    if (act && dim > 2) dprev = cell_diff(S, g, N, spec, i, j, kb - 1, Tg);
+    for (int k = kb; k < ke; ++k)
+    {
+        const double dc = act ? cell_diff(S, g, N, spec, i, j, k, Tg) : 0.0;
+        sd[ty][tx + 1] = dc;
+        if (tx == 0 && j < ny) sd[ty][0] = cell_diff(S, g, N, spec, i - 1, j, k, Tg);
+        if (ty == 0 && i < nx && dim > 1) sy[tx] = cell_diff(S, g, N, spec, i, j - 1, k, Tg);
+        __syncthreads();
+        if (act)
+        {
+            const int nx1 = nx + 1;
+            bx[i + (long long)nx1 * (j + (long long)ny * k)] = hm(sd[ty][tx], dc);
+            if (i == nx - 1)
+                bx[nx + (long long)nx1 * (j + (long long)ny * k)] =
+                    hm(dc, cell_diff(S, g, N, spec, nx, j, k, Tg));
+            if (dim > 1)
+            {
+                const int ny1 = ny + 1;
+                const double dm = ty ? sd[ty - 1][tx + 1] : sy[tx];
+                by[i + (long long)nx * (j + (long long)ny1 * k)] = hm(dm, dc);
+                if (j == ny - 1)
+                    by[i + (long long)nx * (ny + (long long)ny1 * k)] =
+                        hm(dc, cell_diff(S, g, N, spec, i, ny, k, Tg));
+            }
+            if (dim > 2)
+            {
+                const long long t = i + (long long)nx * (j + (long long)ny * k);
+                bz[t] = hm(dprev, dc);
+                if (k == nz - 1)
+                    bz[t + (long long)nx * ny] = hm(dc, cell_diff(S, g, N, spec, i, j, nz, Tg));
+            }
+        }
+        dprev = dc;
+        __syncthreads();
+    }
+}
+
 __global__ void k_species_rhs(GridDev g, GridDev gm, const double* __restrict__ S,
                               const double* __restrict__ Sold, const double* __restrict__ expl,
                               int spec, double dt, double ts, double scale,

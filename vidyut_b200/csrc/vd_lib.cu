@@ -1443,9 +1443,33 @@ void species_setup64(Ctx& c, int comp, double time, const double* Sold, Hier<dou
     const double ts = cfg.time_scale;
     const double scale = (comp == EEN_ID) ? cfg.elecenergy_scale : cfg.species_scale[comp];
     const int* bct = bct_for(c, comp);
-    for (int d = 0; d < cfg.dim; ++d)
-        LAUNCH(k_species_faces, gsz(face_count(c.g, d)), BS, c.st, c.g, d, c.S, comp,
-               cfg.gas_temperature, H.bf[0][d]);
+    const bool faces3 = [] {
+        // VD_SPECIES_FACES3=0: one k_species_faces launch per direction (the
+        // same bits; tests compare the two)
+        const char* e = std::getenv("VD_SPECIES_FACES3");
+        return !(e && e[0] == '0');
+    }();
+    if (!faces3)
+        for (int d = 0; d < cfg.dim; ++d)
+            LAUNCH(k_species_faces, gsz(face_count(c.g, d)), BS, c.st, c.g, d, c.S, comp,
+                   cfg.gas_temperature, H.bf[0][d]);
+    else
+    {
+        // face coefficients of every direction in one pass (k_species_faces3):
+        // 32 x 8 cells a block, z in chunks for about 32 blocks per SM (short
+        // marches: 4, 8, 16, 32 blocks per SM measured 31.0, 30.3, 30.2,
+        // 30.1 ms per 192^3 LMEA step against 32.3 ms for one launch per
+        // direction; the 256^3 Townsend step, whose ion diffusivity is a
+        // constant, within 0.05 ms either way)
+        const int gx = (c.g.n[0] + 31) / 32, gy = (c.g.n[1] + 7) / 8, nz = c.g.n[2];
+        const int chunks =
+            std::max(1, std::min(nz, (32 * sm_count() + gx * gy - 1) / (gx * gy)));
+        const int kchunk = (nz + chunks - 1) / chunks;
+        LAUNCH(k_species_faces3, dim3(gx, gy, (nz + kchunk - 1) / kchunk), 256, c.st, c.g, c.S,
+               comp, cfg.gas_temperature, kchunk, H.bf[0][0],
+               cfg.dim > 1 ? H.bf[0][1] : (double*)nullptr,
+               cfg.dim > 2 ? H.bf[0][2] : (double*)nullptr);
+    }
     LAUNCH(k_species_rhs, gsz(c.N), BS, c.st, c.g, H.g[0], c.S, Sold, c.expl, comp, cfg.dt,
            ts, scale, rhs, c.u[comp]);
     fill_bc(c, 1, comp, bct, 3, 1.0 / scale, time, sides);

@@ -3,6 +3,7 @@
     python -m vidyut_b200.runstep [--n 256] [--warmup 3] [--steps 1] [--fp32] [--warm]
     python -m vidyut_b200.runstep --n 208 --solve           # one field solve
     python -m vidyut_b200.runstep --n 192 --solve --explicit  # + explicit sources
+    python -m vidyut_b200.runstep --lmea --n 192 --steps 1     # the 8-species LMEA step
 
 The workload is the two-species Townsend discharge of ``bench.py``
 (``workloads.townsend_config(3, n)``, seeded initial state 0).  With
@@ -31,6 +32,9 @@ def main() -> None:
     ap.add_argument("--inner", type=int, default=0, help="FP32 V-cycles per refinement pass")
     ap.add_argument("--solve", action="store_true", help="one field solve instead of steps")
     ap.add_argument("--explicit", action="store_true", help="with --solve: explicit sources too")
+    ap.add_argument("--lmea", action="store_true",
+                    help="the 8-species LMEA workload with the electron-energy equation "
+                         "(workloads.lmea_*) instead of the Townsend one")
     ap.add_argument("--mgsolve", action="store_true",
                     help="the solver workload (workloads.mgsolve_*): one warm-up and one "
                          "timed potential solve")
@@ -57,7 +61,7 @@ def main() -> None:
               f"V-cycles {st.iterations}, refinements {st.refinements}")
         g.close()
         return
-    cfg = W.townsend_config(3, a.n)
+    cfg = W.lmea_config(a.n) if a.lmea else W.townsend_config(3, a.n)
     if a.fp32:
         cfg["mg_precision"] = vb.VD_MG_FP32_REFINED
     if a.warm:
@@ -65,7 +69,7 @@ def main() -> None:
     if a.inner > 0:
         cfg["mg_inner_cycles"] = a.inner
     g = vb.Vidyut(cfg)
-    g.set_state(0, W.initial_state(cfg, 0))
+    g.set_state(0, W.lmea_state(cfg, 0) if a.lmea else W.initial_state(cfg, 0))
     if a.solve:
         st = g.solve_potential(0.0)
         if a.explicit:
