@@ -530,6 +530,20 @@ def main():
 
     # roofline of the dominant kernel (fine-level Poisson RB sweep)
     peak, peak_kind = load_peaks()
+
+    # the step's other HBM-bound kernels, each timed live on its own pass
+    # (20 steps) with events around its launches
+    kernels_live = {}
+    for kname, pid in (("k_efield2", vb.VD_PROF_EFIELD),
+                       ("k_poisson_rhs", vb.VD_PROF_POISSON_RHS),
+                       ("k_species_rhs", vb.VD_PROF_SPECIES_RHS)):
+        _, _, (nk, kms, kbytes) = timed(g, min(args.steps, 20), dist, pid)
+        if nk:
+            ks = (kms / nk) / 1e3
+            kernels_live[kname] = {"avg_launch_us": ks * 1e6, "launches_timed": nk,
+                                   "algorithmic_bytes_per_launch": kbytes,
+                                   "achieved_gbs": kbytes / ks / 1e9,
+                                   "frac": kbytes / ks / 1e9 / peak, "peak_kind": peak_kind}
     nl, pms, pbytes = prof
     avg_s = (pms / nl) / 1e3 if nl else float("nan")
     achieved = pbytes / avg_s / 1e9 if nl else None
@@ -652,6 +666,7 @@ def main():
             "gpu_launches": launches,
             "roofline": roof,
             "roofline_explicit": roof_explicit,
+            "kernels_live": kernels_live or None,
             "step_roofline": step_roofline(ms / args.steps, ncell, step_bytes(pv, sv, 2),
                                            peak, peak_kind),
             "cpu_baseline": cpu,

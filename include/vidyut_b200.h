@@ -201,6 +201,9 @@ typedef struct vd_step_stats {
 #define VD_PROF_POISSON_SMOOTH 1     /* FP64 Poisson fine-level RB sweeps   */
 #define VD_PROF_EXPLICIT 2           /* fused reaction + drift-flux kernel   */
 #define VD_PROF_POISSON_SMOOTH32 3   /* FP32 Poisson fine-level RB sweeps   */
+#define VD_PROF_EFIELD 4             /* E = -grad(phi), E/N, potential out   */
+#define VD_PROF_POISSON_RHS 5        /* Poisson right-hand side + guess      */
+#define VD_PROF_SPECIES_RHS 6        /* implicit-diffusion right-hand side   */
 
 /* Reference defaults (Source/Vidyut.H:250-400). */
 vd_status vd_config_init(vd_config* cfg);

@@ -115,6 +115,9 @@ VD_PROF_NONE = 0
 VD_PROF_POISSON_SMOOTH = 1
 VD_PROF_EXPLICIT = 2
 VD_PROF_POISSON_SMOOTH32 = 3
+VD_PROF_EFIELD = 4
+VD_PROF_POISSON_RHS = 5
+VD_PROF_SPECIES_RHS = 6
 
 
 class VidyutError(RuntimeError):

@@ -361,10 +361,42 @@ __global__ void __launch_bounds__(128) k_efield2(GradCtx C, const double* __rest
     const long long N = g.ncell();
     const long long t = i + (long long)g.n[0] * (j + (long long)g.n[1] * k);
     double x0[2], E[2][3];
+    const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+    if (g.rb && g.dim == 3 && i >= 2 && i + 2 < nx && j > 0 && j < ny - 1 && k > 0 && k < nz - 1)
+    {
+        // interior pair on the red-black split potential: cell i is of
+        // colour c0 = (i+j+k) & 1 and cell i+1 of the other, both at
+        // half-index h; every neighbour is a fixed offset from h in one of
+        // the two halves (x: i-1 and i+2 at h-1 and h+1; y, z: +-row, +-plane)
+        const int nxh = nx >> 1, c0 = (i + j + k) & 1;
+        const long long half = g.ncell() >> 1, row = nxh, plane = (long long)nxh * ny;
+        const long long h = (i >> 1) + nxh * (j + (long long)ny * k);
+        const double* __restrict__ sa = sol + c0 * half;       // colour of cell i
+        const double* __restrict__ sb = sol + (1 - c0) * half; // colour of cell i+1
+        x0[0] = sa[h];
+        x0[1] = sb[h];
+        const double nA[6] = {sb[h - 1], x0[1], sb[h - row], sb[h + row], sb[h - plane],
+                              sb[h + plane]};
+        const double nB[6] = {x0[0], sa[h + 1], sa[h - row], sa[h + row], sa[h - plane],
+                              sa[h + plane]};
 #pragma unroll
-    for (int e = 0; e < 2; ++e) x0[e] = sol[g.idx(i + e, j, k)];
+        for (int d = 0; d < 3; ++d)
+        {
+            // efield_cell's interior arithmetic
+            const double gla = (x0[0] - nA[2 * d]) * C.dxi[d];
+            const double gha = (nA[2 * d + 1] - x0[0]) * C.dxi[d];
+            E[0][d] = 0.5 * (gla * (-1.0 * ps) + gha * (-1.0 * ps));
+            const double glb = (x0[1] - nB[2 * d]) * C.dxi[d];
+            const double ghb = (nB[2 * d + 1] - x0[1]) * C.dxi[d];
+            E[1][d] = 0.5 * (glb * (-1.0 * ps) + ghb * (-1.0 * ps));
+        }
+    } else
+    {
 #pragma unroll
-    for (int e = 0; e < 2; ++e) efield_cell(C, sol, i + e, j, k, x0[e], ps, E[e]);
+        for (int e = 0; e < 2; ++e) x0[e] = sol[g.idx(i + e, j, k)];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) efield_cell(C, sol, i + e, j, k, x0[e], ps, E[e]);
+    }
     for (int d = 0; d < g.dim; ++d)
         *reinterpret_cast<double2*>(S + (EFX_ID + d) * N + t) = make_double2(E[0][d], E[1][d]);
     double nd[2] = {0.0, 0.0};

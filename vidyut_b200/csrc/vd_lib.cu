@@ -1259,8 +1259,22 @@ void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats,
 {
     const vd_config& cfg = c.cfg;
     const double ps = cfg.potential_scale;
+    const bool prof_rhs = t_prof && t_prof->id == VD_PROF_POISSON_RHS;
+    if (prof_rhs)
+    {
+        // reads the charged species (and the coupling source, the last
+        // potential when warm), writes the right-hand side and the guess
+        int kc[NUM_SPECIES];
+        CKCHRG(kc);
+        int nq = 0;
+        for (int sp = 0; sp < NUM_SPECIES; ++sp) nq += (kc[sp] != 0 && cfg.do_spacechrg) ? 1 : 0;
+        const int nin = nq + (ephi ? 1 : 0) + (cfg.poisson_warm_start ? 1 : 0);
+        t_prof->bytes = 8.0 * (nin + 2) * (double)c.N;
+        t_prof->begin(c.st);
+    }
     LAUNCH(k_poisson_rhs, gsz(c.N), BS, c.st, c.G, c.HP.g[0], Sold, c.S, c.phi_rhs, c.phi_sol,
            cfg.do_spacechrg, cfg.poisson_warm_start, ps, time, c.dpp, ephi);
+    if (prof_rhs) t_prof->end(c.st);
     fill_bc(c, 0, POT_ID, c.pbct, 2, 1.0 / ps, time, c.pside);
     if (c.HP.varb)
     {
@@ -1304,11 +1318,20 @@ void poisson(Ctx& c, double time, const double* Sold, vd_solve_stats* stats,
     c.poisson_refs += st.refinements;
     c.max_poisson_res = std::max(c.max_poisson_res, st.final_residual);
     if (stats) *stats = st;
+    const bool prof_ef = t_prof && t_prof->id == VD_PROF_EFIELD;
+    if (prof_ef)
+    {
+        // reads the potential and every species, writes E (dim), E/N and
+        // the potential
+        t_prof->bytes = 8.0 * (1 + NUM_SPECIES + cfg.dim + 2) * (double)c.N;
+        t_prof->begin(c.st);
+    }
     if (c.g.n[0] % 2 == 0)
     {
         // two cells per thread, 16-byte state accesses
         const dim3 grid((c.g.n[0] / 2 + 127) / 128, c.g.n[1], c.g.n[2]);
         LAUNCH(k_efield2, grid, 128, c.st, grad_ctx(c, c.HP, c.pside), c.phi_sol, c.S, ps);
+        if (prof_ef) t_prof->end(c.st);
     } else
     {
         const Grid3 ge = rows3(c.g);
@@ -1470,8 +1493,17 @@ void species_setup64(Ctx& c, int comp, double time, const double* Sold, Hier<dou
                cfg.dim > 1 ? H.bf[0][1] : (double*)nullptr,
                cfg.dim > 2 ? H.bf[0][2] : (double*)nullptr);
     }
+    const bool prof_srhs = t_prof && t_prof->id == VD_PROF_SPECIES_RHS;
+    if (prof_srhs)
+    {
+        // reads the old and current density and the explicit source, writes
+        // the right-hand side and the initial guess
+        t_prof->bytes = 8.0 * 5 * (double)c.N;
+        t_prof->begin(c.st);
+    }
     LAUNCH(k_species_rhs, gsz(c.N), BS, c.st, c.g, H.g[0], c.S, Sold, c.expl, comp, cfg.dt,
            ts, scale, rhs, c.u[comp]);
+    if (prof_srhs) t_prof->end(c.st);
     fill_bc(c, 1, comp, bct, 3, 1.0 / scale, time, sides);
     hier_set_ops(H, (1.0 / cfg.dt) * ts * 1.0, ts, 1.0, bct, 3);
     hier_coarsen_coeffs(H, bct, c.st);
