@@ -1058,64 +1058,101 @@ __device__ __forceinline__ double onesided_grad(const double* S, const GridDev& 
     return 2.0 * g1 - g2;
 }
 
-__global__ void k_joule(JouleParams P)
+// The Joule term of one face (d, face): q (mu n_e E_f - D grad n_e) E_f with
+// the face averages of Te, |E|, n_e and the total density, the face field
+// from the potential and the face gradient of the electron solution (one-sided
+// at the domain ends) -- a function of the face alone
+// (Source/ElecEnergySource.cpp:149-273).
+__device__ __forceinline__ double joule_face(const JouleParams& P, const GridDev& g, long long N,
+                                             int d, const int* face)
+{
+    const double* __restrict__ S = P.S;
+    const double charge = plasmachem::get_charge(P.eidx) * ECHARGE;
+    int lc[3] = {face[0], face[1], face[2]};
+    lc[d] -= 1;
+    const long long ql = g.idx(clampi(lc[0], g.n[0], g.per[0]), clampi(lc[1], g.n[1], g.per[1]),
+                               clampi(lc[2], g.n[2], g.per[2]));
+    const long long qr = g.idx(clampi(face[0], g.n[0], g.per[0]),
+                               clampi(face[1], g.n[1], g.per[1]),
+                               clampi(face[2], g.n[2], g.per[2]));
+    const double te = (S[ETEMP_ID * N + ql] + S[ETEMP_ID * N + qr]) / 2.0;
+    double Esum = 0.0;
+    for (int q = 0; q < g.dim; ++q)
+    {
+        const double e = (S[(EFX_ID + q) * N + ql] + S[(EFX_ID + q) * N + qr]) / 2.0;
+        Esum += e * e;
+    }
+    const double emag = sqrt(Esum);
+    const double ne = (S[P.eidx * N + ql] + S[P.eidx * N + qr]) / 2.0;
+    const double ef = grad_at_face(P.pot, P.phi_sol, d, face[0], face[1], face[2]) * (-1.0 * P.ps);
+    double nd = 0.0;
+#pragma unroll
+    for (int sp = 0; sp < NUM_SPECIES; sp++) nd += (S[sp * N + ql] + S[sp * N + qr]) / 2.0;
+    const double mu = specMob(P.eidx, te, nd, emag, P.Tg);
+    const double dc = specDiff(P.eidx, te, nd, emag, P.Tg);
+    double gn;
+    if (face[d] == 0 || face[d] == g.n[d])
+    {
+        const int sgn = (face[d] == 0) ? -1 : 1;
+        gn = onesided_grad(S, g, N, P.eidx, face, sgn, d, P.dx[d]);
+    } else
+    {
+        gn = (P.ue[P.gm.idx(face[0], face[1], face[2])] - P.ue[P.gm.idx(lc[0], lc[1], lc[2])]) *
+             (1.0 / P.dx[d]) * P.escale;
+    }
+    const double cd = charge * (mu * ne * ef - dc * gn);
+    return cd * ef;
+}
+
+// Joule heating of every cell (compute_elecenergy_source's jh: half the sum
+// of its faces' terms, x-lo, x-hi, y-lo, y-hi, z-lo, z-hi, floored at zero
+// when asked) in two passes: every face's term once into a face array --
+// evaluated per cell, each interior face costs twice its ~30 state loads and
+// two transport-hook calls -- then the per-cell sums in that order.  The
+// product of a face term is rounded before the sum, as the oracle does.
+__global__ void k_joule_faces(JouleParams P, int d, double* __restrict__ pf)
 {
     VD_PDL_WAIT();
-    // the state is in natural layout; the Poisson level's grid may be red-black
     GridDev g = P.pot.op.g;
     g.rb = 0;
     const long long N = g.ncell();
-    const double* __restrict__ S = P.S;
+    const long long tot = face_count(g, d);
+    const int nx = g.n[0] + (d == 0), ny = g.n[1] + (d == 1);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        int face[3];
+        face[0] = (int)(t % nx);
+        const long long r = t / nx;
+        face[1] = (int)(r % ny);
+        face[2] = (int)(r / ny);
+        pf[t] = joule_face(P, g, N, d, face);
+    }
+}
+
+__global__ void k_joule_sum(JouleParams P, const double* __restrict__ px,
+                            const double* __restrict__ py, const double* __restrict__ pz)
+{
+    VD_PDL_WAIT();
+    GridDev g = P.pot.op.g;
+    g.rb = 0;
+    const long long N = g.ncell();
+    const int nx = g.n[0], ny = g.n[1];
+    const double* pfs[3] = {px, py, pz};
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
          t += (long long)gridDim.x * blockDim.x)
     {
         int c3[3];
         cell_of(g, t, c3[0], c3[1], c3[2]);
-        const double charge = plasmachem::get_charge(P.eidx) * ECHARGE;
         double jh = 0.0;
         for (int d = 0; d < g.dim; ++d)
-            for (int f = 0; f < 2; ++f)
-            {
-                int face[3] = {c3[0], c3[1], c3[2]};
-                face[d] += f;
-                int lc[3] = {face[0], face[1], face[2]};
-                lc[d] -= 1;
-                const long long ql = g.idx(clampi(lc[0], g.n[0], g.per[0]),
-                                           clampi(lc[1], g.n[1], g.per[1]),
-                                           clampi(lc[2], g.n[2], g.per[2]));
-                const long long qr = g.idx(clampi(face[0], g.n[0], g.per[0]),
-                                           clampi(face[1], g.n[1], g.per[1]),
-                                           clampi(face[2], g.n[2], g.per[2]));
-                const double te = (S[ETEMP_ID * N + ql] + S[ETEMP_ID * N + qr]) / 2.0;
-                double Esum = 0.0;
-                for (int q = 0; q < g.dim; ++q)
-                {
-                    const double e = (S[(EFX_ID + q) * N + ql] + S[(EFX_ID + q) * N + qr]) / 2.0;
-                    Esum += e * e;
-                }
-                const double emag = sqrt(Esum);
-                const double ne = (S[P.eidx * N + ql] + S[P.eidx * N + qr]) / 2.0;
-                const double ef =
-                    grad_at_face(P.pot, P.phi_sol, d, face[0], face[1], face[2]) * (-1.0 * P.ps);
-                double nd = 0.0;
-#pragma unroll
-                for (int sp = 0; sp < NUM_SPECIES; sp++) nd += (S[sp * N + ql] + S[sp * N + qr]) / 2.0;
-                const double mu = specMob(P.eidx, te, nd, emag, P.Tg);
-                const double dc = specDiff(P.eidx, te, nd, emag, P.Tg);
-                double gn;
-                if (face[d] == 0 || face[d] == g.n[d])
-                {
-                    const int sgn = (face[d] == 0) ? -1 : 1;
-                    gn = onesided_grad(S, g, N, P.eidx, face, sgn, d, P.dx[d]);
-                } else
-                {
-                    gn = (P.ue[P.gm.idx(face[0], face[1], face[2])] -
-                          P.ue[P.gm.idx(lc[0], lc[1], lc[2])]) *
-                         (1.0 / P.dx[d]) * P.escale;
-                }
-                const double cd = charge * (mu * ne * ef - dc * gn);
-                jh += cd * ef;
-            }
+        {
+            const int fx = nx + (d == 0), fy = ny + (d == 1);
+            const long long lo = c3[0] + (long long)fx * (c3[1] + (long long)fy * c3[2]);
+            const long long step = (d == 0) ? 1 : ((d == 1) ? fx : (long long)fx * fy);
+            jh += pfs[d][lo];
+            jh += pfs[d][lo + step];
+        }
         jh *= 0.5;
         if (P.floor_jh && jh < 0.0) jh = 0.0;
         P.expl[NUM_SPECIES * N + t] += jh;

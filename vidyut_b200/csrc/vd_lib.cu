@@ -810,6 +810,7 @@ struct Ctx
     double* expl = nullptr;
     double* rxn_een = nullptr;
     double* ejh = nullptr;
+    double* jface[3] = {};   // Joule term of every face, per direction (energy equation)
     double* u[VD_NT] = {};   // solve outputs, indexed by component
     double* phi_sol = nullptr;
     double* phi_rhs = nullptr;
@@ -1649,7 +1650,9 @@ void joule(Ctx& c)
     P.Tg = c.cfg.gas_temperature;
     P.floor_jh = c.cfg.floor_jh;
     P.eidx = c.eidx;
-    LAUNCH(k_joule, gsz(c.N), BS, c.st, P);
+    for (int d = 0; d < c.cfg.dim; ++d)
+        LAUNCH(k_joule_faces, gsz(face_count(c.g, d)), BS, c.st, P, d, c.jface[d]);
+    LAUNCH(k_joule_sum, gsz(c.N), BS, c.st, P, c.jface[0], c.jface[1], c.jface[2]);
 }
 
 FinalParams final_params(Ctx& c)
@@ -2338,6 +2341,8 @@ vd_status vd_create(const vd_config* cfg, void** out)
         VD_CUDA_OK(cudaMemset(c->expl, 0, sizeof(double) * (size_t)VD_NT * N));
         c->rxn_een = c->A.get<double>(N);
         c->ejh = c->A.get<double>(N);
+        if (cfg->elecenergy_solve)
+            for (int d = 0; d < c->cfg.dim; ++d) c->jface[d] = c->A.get<double>(face_count(c->g, d));
         // a solution array per species (background ones too: a
         // multicomponent chunk or vd_implicit_diffusion_chunk may solve them)
         for (int sp = 0; sp < NUM_SPECIES; ++sp) c->u[sp] = c->A.get<double>(N);
