@@ -15,9 +15,11 @@
 //
 // Backward step k (lambda = dJ/du^{k+1}, states recomputed from checkpoints):
 //     lambda <- lambda + dt (dR/du)^T lambda,   g <- g + dt (dR/dp)^T lambda
-// evaluated at u^k.  One thread per face differentiates its flux with dual
-// numbers (one pass for the stencil densities, one for the velocities) and
-// scatters w dF/du_m with FP64 atomics, w = dt (lambda_R - lambda_L)/dx.
+// evaluated at u^k.  One thread per face differentiates its flux -- WENO:
+// from the 5-slot dual gradient of each of its four reconstructions
+// (weno_face_flux_grad); upwind and WAF: dual numbers, one pass for the
+// stencil densities and one for the velocities -- and scatters w dF/du_m
+// with FP64 atomics, w = dt (lambda_R - lambda_L)/dx.
 // Stencil positions that clamp onto the same boundary cell are seeded as one
 // direction: the WENO smoothness indicators of such a flat sub-stencil are
 // zero only up to rounding, and per-position derivatives of that rounding
@@ -109,6 +111,93 @@ __device__ __forceinline__ R face_flux_T(const R* u, const R* v, int hyp_order,
     const R uph = weno5_T(u[0], u[1], u[2], u[3], u[4], weno_scheme);
     const R umh = weno5_T(u[5], u[4], u[3], u[2], u[1], weno_scheme);
     return 0.5 * (fph + lam * uph) + 0.5 * (fmh - lam * umh);
+}
+
+// Value and gradient of one WENO5 reconstruction with respect to its five
+// cells (forward mode over 5 slots).  Arguments that are one cell (stencil
+// positions clamped onto the same boundary cell) share the slot of the first
+// of them, grp[k] <= k, so they move together: the smoothness indicator of a
+// flat sub-stencil then has an exactly zero derivative, instead of
+// per-position derivatives of its rounding residue, amplified by
+// 1/(beta + eps)^2, that do not cancel.  g[k] is set for k == grp[k].
+__device__ __forceinline__ double weno5_grad(const double* x, const int* grp, int scheme,
+                                             double* g)
+{
+    const Dual<5> W = weno5_T(Dual<5>::var(x[0], grp[0]), Dual<5>::var(x[1], grp[1]),
+                              Dual<5>::var(x[2], grp[2]), Dual<5>::var(x[3], grp[3]),
+                              Dual<5>::var(x[4], grp[4]), scheme);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) g[k] = W.d[k];
+    return W.v;
+}
+
+// Derivatives of the WENO face flux (face_flux_T, hyp_order > 2) with respect
+// to the densities (du) and drift velocities (dv) of the cells of its
+// stencil, accumulated at each cell's first stencil position (dir[m]: the
+// first position clamped onto the cell of position m).  With f_m = u_m v_m
+// and lam = |(v_2 + v_3)/2|:
+//   F = (fph + lam uph)/2 + (fmh - lam umh)/2,
+//   dF/du = dF/df v + lam (duph/du - dumh/du)/2,
+//   dF/dv = dF/df u + (uph - umh)/2 dlam/dv   (dlam/dv only at positions 2, 3).
+// Four 5-slot reconstructions instead of the two passes of four 6-slot ones
+// that differentiate face_flux_T in dual numbers; the same derivatives up to
+// rounding, with the same seeding of clamped positions.
+__device__ __forceinline__ void weno_face_flux_grad(const double* u, const double* v,
+                                                    const int* dir, int scheme, double* du,
+                                                    double* dv)
+{
+    // argument positions of the reconstructions: fph, uph over 0..4; fmh, umh
+    // over 5, 4, 3, 2, 1; and each argument's slot (its group's first argument)
+    const int pp[5] = {0, 1, 2, 3, 4}, pm[5] = {5, 4, 3, 2, 1};
+    int gpp[5], gpm[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+    {
+        gpp[k] = k;
+        gpm[k] = k;
+        for (int q = k - 1; q >= 0; --q)
+        {
+            if (dir[pp[q]] == dir[pp[k]]) gpp[k] = gpp[q];
+            if (dir[pm[q]] == dir[pm[k]]) gpm[k] = gpm[q];
+        }
+    }
+    double xf[5], xu[5], yf[5], yu[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+    {
+        xf[k] = u[pp[k]] * v[pp[k]];
+        xu[k] = u[pp[k]];
+        yf[k] = u[pm[k]] * v[pm[k]];
+        yu[k] = u[pm[k]];
+    }
+    double gfp[5], gfm[5], gup[5], gum[5];
+    weno5_grad(xf, gpp, scheme, gfp);
+    weno5_grad(yf, gpm, scheme, gfm);
+    const double uph = weno5_grad(xu, gpp, scheme, gup);
+    const double umh = weno5_grad(yu, gpm, scheme, gum);
+    const double vm = 0.5 * (v[2] + v[3]);
+    const double lam = (vm < 0.0) ? -vm : vm, slam = (vm < 0.0) ? -1.0 : 1.0;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) du[m] = dv[m] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+    {
+        if (gpp[k] == k)
+        {
+            const int c = dir[pp[k]], m = pp[k];
+            du[c] += 0.5 * gfp[k] * v[m] + 0.5 * lam * gup[k];
+            dv[c] += 0.5 * gfp[k] * u[m];
+        }
+        if (gpm[k] == k)
+        {
+            const int c = dir[pm[k]], m = pm[k];
+            du[c] += 0.5 * gfm[k] * v[m] - 0.5 * lam * gum[k];
+            dv[c] += 0.5 * gfm[k] * u[m];
+        }
+    }
+    const double dl = 0.5 * (uph - umh) * slam * 0.5;
+    dv[dir[2]] += dl;
+    dv[dir[3]] += dl;
 }
 
 #ifdef VD_HAS_MECH_ADJOINT
@@ -268,6 +357,24 @@ __global__ void __launch_bounds__(128) k_adj_faces(AdjParams P, int d,
             {
                 uv[m] = u[s * N + qm[m]];
                 vv[m] = P.mu[s * N + qm[m]] * P.S[(EFX_ID + d) * N + qm[m]];
+            }
+            if (P.hyp_order > 2)
+            {
+                // WENO: both derivative sets from one gradient per
+                // reconstruction, at each cell's first stencil position
+                double au[6], av[6];
+                weno_face_flux_grad(uv, vv, dir, P.weno_scheme, au, av);
+                for (int m = 0; m < 6; ++m)
+                {
+                    if (dir[m] != m) continue;
+                    if (au[m] != 0.0) atomicAdd(&adj[s * N + qm[m]], w * au[m]);
+                    if (av[m] == 0.0) continue;
+                    const double e = P.S[(EFX_ID + d) * N + qm[m]];
+                    const double dn = P.dmu[s * N + qm[m]] * e;
+                    if (dn != 0.0) atomicAdd(&adjnd[qm[m]], w * av[m] * dn);
+                    if (s == P.eslot) gm += w * av[m] * vv[m];
+                }
+                continue;
             }
             {
                 Dual<6> U[6], V[6];
