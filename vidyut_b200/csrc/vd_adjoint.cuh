@@ -202,6 +202,14 @@ __device__ __forceinline__ void weno_face_flux_grad(const double* u, const doubl
 
 #ifdef VD_HAS_MECH_ADJOINT
 
+// columns of the chemistry Jacobian formed per dual pass (k_adj_chem_update):
+// each pass recomputes the rate exponentials, more slots cost registers;
+// measured at 128^3 / 50 steps (LMEA): 1, 2, 4, 8 slots 1033, 1002, 1048,
+// 1038 ms per adjoint run
+#ifndef VD_ADJ_CHEM_SLOTS
+#define VD_ADJ_CHEM_SLOTS 2
+#endif
+
 struct AdjParams
 {
     GridDev g; // natural layout
@@ -446,18 +454,24 @@ __global__ void __launch_bounds__(128) k_adj_chem_update(AdjParams P,
             mech_lam_nu(lamc, ln);
             for (int r = 0; r < NUM_REACTIONS; ++r) gl[r] += P.dt * N_A * q[r] * ln[r];
         }
-        // dR_s/du_s2 = d wdot_s / d C_s2 (R = N_A wdot, C = u / N_A), one column per pass
+        // dR_s/du_s2 = d wdot_s / d C_s2 (R = N_A wdot, C = u / N_A),
+        // VD_ADJ_CHEM_SLOTS columns per pass
         const double nd = adjnd[t];
-        for (int s2 = 0; s2 < P.nt; ++s2)
+        constexpr int K = VD_ADJ_CHEM_SLOTS;
+        for (int s0 = 0; s0 < P.nt; s0 += K)
         {
-            Dual<1> C[NUM_SPECIES], q[NUM_REACTIONS], W[NUM_SPECIES];
-            for (int sp = 0; sp < NUM_SPECIES; ++sp) C[sp] = Dual<1>(Cv[sp]);
-            C[P.spec[s2]].d[0] = 1.0;
-            mech_rates<Dual<1>>(P.Tg, C, te, P.theta, q);
-            mech_wdot<Dual<1>>(q, W);
-            double a = 0.0;
-            for (int sp = 0; sp < NUM_SPECIES; ++sp) a += lamc[sp] * W[sp].d[0];
-            lam[s2 * N + t] = lamc[P.spec[s2]] + P.dt * a + adj[s2 * N + t] + nd;
+            Dual<K> C[NUM_SPECIES], q[NUM_REACTIONS], W[NUM_SPECIES];
+            for (int sp = 0; sp < NUM_SPECIES; ++sp) C[sp] = Dual<K>(Cv[sp]);
+            for (int e = 0; e < K && s0 + e < P.nt; ++e) C[P.spec[s0 + e]].d[e] = 1.0;
+            mech_rates<Dual<K>>(P.Tg, C, te, P.theta, q);
+            mech_wdot<Dual<K>>(q, W);
+            for (int e = 0; e < K && s0 + e < P.nt; ++e)
+            {
+                const int s2 = s0 + e;
+                double a = 0.0;
+                for (int sp = 0; sp < NUM_SPECIES; ++sp) a += lamc[sp] * W[sp].d[e];
+                lam[s2 * N + t] = lamc[P.spec[s2]] + P.dt * a + adj[s2 * N + t] + nd;
+            }
         }
     }
     for (int r = 0; r < NUM_REACTIONS; ++r)
