@@ -4,6 +4,7 @@
     python -m vidyut_b200.runstep --n 208 --solve           # one field solve
     python -m vidyut_b200.runstep --n 192 --solve --explicit  # + explicit sources
     python -m vidyut_b200.runstep --lmea --n 192 --steps 1     # the 8-species LMEA step
+    python -m vidyut_b200.runstep --adjoint --n 128 --steps 50 # the discrete adjoint
 
 The workload is the two-species Townsend discharge of ``bench.py``
 (``workloads.townsend_config(3, n)``, seeded initial state 0).  With
@@ -35,6 +36,9 @@ def main() -> None:
     ap.add_argument("--lmea", action="store_true",
                     help="the 8-species LMEA workload with the electron-energy equation "
                          "(workloads.lmea_*) instead of the Townsend one")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="the discrete-adjoint workload (workloads.adjoint_*): one warm-up "
+                         "and one timed checkpointed adjoint run of --steps explicit steps")
     ap.add_argument("--mgsolve", action="store_true",
                     help="the solver workload (workloads.mgsolve_*): one warm-up and one "
                          "timed potential solve")
@@ -43,6 +47,20 @@ def main() -> None:
     import vidyut_b200 as vb
     from vidyut_b200 import workloads as W
 
+    if a.adjoint:
+        import time
+        cfg = W.adjoint_config(a.n)
+        g = vb.Vidyut(cfg)
+        g.set_state(0, W.adjoint_state(cfg, 0))
+        g.adjoint_run(5, K=5)
+        l0 = g.launch_count()
+        t0 = time.perf_counter()
+        J, grad = g.adjoint_run(a.steps, K=10)
+        el = time.perf_counter() - t0
+        print(f"timed adjoint run of {a.steps} steps: {g.launch_count() - l0} launches, "
+              f"{1e3 * el:.3f} ms, J {J:.6e}")
+        g.close()
+        return
     if a.mgsolve:
         import time
         cfg = W.mgsolve_config(a.n)
