@@ -38,7 +38,8 @@ def main() -> None:
                          "(workloads.lmea_*) instead of the Townsend one")
     ap.add_argument("--adjoint", action="store_true",
                     help="the discrete-adjoint workload (workloads.adjoint_*): one warm-up "
-                         "and one timed checkpointed adjoint run of --steps explicit steps")
+                         "and one timed checkpointed adjoint run of --steps explicit steps, "
+                         "K = 10")
     ap.add_argument("--mgsolve", action="store_true",
                     help="the solver workload (workloads.mgsolve_*): one warm-up and one "
                          "timed potential solve")
@@ -52,7 +53,7 @@ def main() -> None:
         cfg = W.adjoint_config(a.n)
         g = vb.Vidyut(cfg)
         g.set_state(0, W.adjoint_state(cfg, 0))
-        g.adjoint_run(5, K=5)
+        g.adjoint_run(a.steps, K=10)  # warm-up of the timed shape: slots allocated
         l0 = g.launch_count()
         t0 = time.perf_counter()
         J, grad = g.adjoint_run(a.steps, K=10)
