@@ -132,6 +132,59 @@ def test_adjoint_vs_tlm(require_gpu, hyp_order, weno):
     assert worst <= 1e-9, worst
 
 
+def periodic_walled(cfg):
+    """x periodic; walls that zero the flux (IHNEUBC) on the ions' z-lo and
+    the electrons' y-hi sides."""
+    cfg["is_periodic"] = [1, 0, 0]
+    cfg["pot_bc_lo"] = [0, 2, 1]
+    cfg["pot_bc_hi"] = [0, 2, 1]
+    for key in ("eden", "ion", "neutral", "eenrg"):
+        cfg[f"{key}_bc_lo"] = [0, 2, 3 if key == "ion" else 2]
+        cfg[f"{key}_bc_hi"] = [0, 3 if key == "eden" else 2, 2]
+    return cfg
+
+
+# The WENO face adjoint by line march (k_adj_faces_line, the default) and by
+# one thread per face (VD_ADJ_FACES_LINE=0): the same derivatives summed in
+# another order; and the line march against the oracle's tangent-linear
+# gradient with a periodic direction and flux-zeroing walls.
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["box", "periodic_walled", "2d"])
+def test_adjoint_face_line_march(require_gpu, monkeypatch, kind):
+    if kind == "2d":
+        cfg = W.adjoint_config(12, prob_hi=[2e-4, 2e-4, 2e-4], dt=5e-12)
+        cfg["dim"] = 2
+        cfg["n_cell"] = [16, 12, 1]
+        cfg["prob_hi"] = [2e-4, 1.5e-4, 1.0]
+        cfg["pot_bc_lo"] = [2, 1, 2]
+        cfg["pot_bc_hi"] = [2, 1, 2]
+        cfg["voltage_amp_hi"] = [0.0, 20e3, 0.0]
+        S = W.adjoint_state(cfg, 4, efield=5e6)
+    else:
+        cfg, S = small_case(n=10 if kind == "periodic_walled" else 12)
+        if kind == "periodic_walled":
+            periodic_walled(cfg)
+    p = params(5)
+    runs = []
+    for v in ("1", "0"):
+        monkeypatch.setenv("VD_ADJ_FACES_LINE", v)
+        g = vb.Vidyut(cfg)
+        g.set_state(0, S)
+        g.adjoint_set_params(p)
+        runs.append(g.adjoint_run(6, K=4))
+        g.close()
+    (J1, g1), (J0, g0) = runs
+    assert J1 == J0
+    worst, _ = grad_close(g1, g0, 1e-12)
+    assert worst <= 1e-12, worst
+    o = Oracle(cfg)
+    o.set_state(0, S)
+    Jo, go = o.adjoint_tlm(6, p)
+    assert abs(J1 - Jo) <= 1e-12 * abs(Jo)
+    worst, _ = grad_close(g1, go, 1e-9)
+    assert worst <= 1e-9, worst
+
+
 @pytest.mark.gpu
 def test_adjoint_checkpoint_intervals(require_gpu):
     cfg, S = small_case()

@@ -123,9 +123,9 @@ __device__ __forceinline__ R face_flux_T(const R* u, const R* v, int hyp_order,
 __device__ __forceinline__ double weno5_grad(const double* x, const int* grp, int scheme,
                                              double* g)
 {
-    const Dual<5> W = weno5_T(Dual<5>::var(x[0], grp[0]), Dual<5>::var(x[1], grp[1]),
-                              Dual<5>::var(x[2], grp[2]), Dual<5>::var(x[3], grp[3]),
-                              Dual<5>::var(x[4], grp[4]), scheme);
+    const Dual<5> W = weno5_T(Dual<5>::var_sel(x[0], grp[0]), Dual<5>::var_sel(x[1], grp[1]),
+                              Dual<5>::var_sel(x[2], grp[2]), Dual<5>::var_sel(x[3], grp[3]),
+                              Dual<5>::var_sel(x[4], grp[4]), scheme);
 #pragma unroll
     for (int k = 0; k < 5; ++k) g[k] = W.d[k];
     return W.v;
@@ -141,7 +141,10 @@ __device__ __forceinline__ double weno5_grad(const double* x, const int* grp, in
 //   dF/dv = dF/df u + (uph - umh)/2 dlam/dv   (dlam/dv only at positions 2, 3).
 // Four 5-slot reconstructions instead of the two passes of four 6-slot ones
 // that differentiate face_flux_T in dual numbers; the same derivatives up to
-// rounding, with the same seeding of clamped positions.
+// rounding, with the same seeding of clamped positions.  ID: no position is
+// clamped (dir[m] == m, an interior face), so every slot and output index is
+// a compile-time constant and the duals stay in registers.
+template <bool ID = false>
 __device__ __forceinline__ void weno_face_flux_grad(const double* u, const double* v,
                                                     const int* dir, int scheme, double* du,
                                                     double* dv)
@@ -155,7 +158,7 @@ __device__ __forceinline__ void weno_face_flux_grad(const double* u, const doubl
     {
         gpp[k] = k;
         gpm[k] = k;
-        for (int q = k - 1; q >= 0; --q)
+        for (int q = k - 1; q >= 0 && !ID; --q)
         {
             if (dir[pp[q]] == dir[pp[k]]) gpp[k] = gpp[q];
             if (dir[pm[q]] == dir[pm[k]]) gpm[k] = gpm[q];
@@ -182,22 +185,40 @@ __device__ __forceinline__ void weno_face_flux_grad(const double* u, const doubl
 #pragma unroll
     for (int k = 0; k < 5; ++k)
     {
-        if (gpp[k] == k)
+        // output index c = dir[m] by a select per position (an indexed
+        // update would put du, dv in local memory)
+        if (ID || gpp[k] == k)
         {
-            const int c = dir[pp[k]], m = pp[k];
-            du[c] += 0.5 * gfp[k] * v[m] + 0.5 * lam * gup[k];
-            dv[c] += 0.5 * gfp[k] * u[m];
+            const int m = pp[k], c = ID ? m : dir[m];
+            const double a = 0.5 * gfp[k] * v[m] + 0.5 * lam * gup[k], b = 0.5 * gfp[k] * u[m];
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+                if (q == c)
+                {
+                    du[q] += a;
+                    dv[q] += b;
+                }
         }
-        if (gpm[k] == k)
+        if (ID || gpm[k] == k)
         {
-            const int c = dir[pm[k]], m = pm[k];
-            du[c] += 0.5 * gfm[k] * v[m] - 0.5 * lam * gum[k];
-            dv[c] += 0.5 * gfm[k] * u[m];
+            const int m = pm[k], c = ID ? m : dir[m];
+            const double a = 0.5 * gfm[k] * v[m] - 0.5 * lam * gum[k], b = 0.5 * gfm[k] * u[m];
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+                if (q == c)
+                {
+                    du[q] += a;
+                    dv[q] += b;
+                }
         }
     }
     const double dl = 0.5 * (uph - umh) * slam * 0.5;
-    dv[dir[2]] += dl;
-    dv[dir[3]] += dl;
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+    {
+        if (q == (ID ? 2 : dir[2])) dv[q] += dl;
+        if (q == (ID ? 3 : dir[3])) dv[q] += dl;
+    }
 }
 
 #ifdef VD_HAS_MECH_ADJOINT
@@ -413,6 +434,144 @@ __global__ void __launch_bounds__(128) k_adj_faces(AdjParams P, int d,
                 }
             }
         }
+    }
+    gm = block_sum(gm, sh);
+    if (threadIdx.x == 0 && gm != 0.0) atomicAdd(gmob, gm / P.mob_scale);
+}
+
+// Adjoint of the WENO face fluxes of direction d (hyp_order > 2): one thread
+// per line of faces along d and species.  The thread marches its line with
+// the six stencil cells' u, v and their accumulated w dF/du, w dF/dv in
+// registers (position m of face f is the virtual cell f-3+m; ghost positions
+// read the clamped or wrapped cell, as k_adj_faces does) and writes each
+// cell's totals once, when it leaves the stencil: adj by a plain add (no
+// other thread of the launch reaches this species' cells of the line),
+// adjnd, which every species shares, by an atomic add.  The derivatives are
+// k_adj_faces' (weno_face_flux_grad with the same grouping of clamped
+// positions), summed per cell before the product with dmu E; each new face
+// loads one new cell instead of six.
+__device__ __forceinline__ void adj_line_flush(double* __restrict__ as, double* __restrict__ adjnd,
+                                               const double* __restrict__ dms,
+                                               const double* __restrict__ E, long long q,
+                                               double au, double av, double v, bool elec,
+                                               double& gm)
+{
+    if (au != 0.0) as[q] += au;
+    if (av == 0.0) return;
+    const double dn = dms[q] * E[q];
+    if (dn != 0.0) atomicAdd(&adjnd[q], av * dn);
+    if (elec) gm += av * v;
+}
+
+__global__ void __launch_bounds__(128) k_adj_faces_line(AdjParams P, int d,
+                                                        const double* __restrict__ u,
+                                                        const double* __restrict__ lam,
+                                                        double* __restrict__ adj,
+                                                        double* __restrict__ adjnd, double* gmob)
+{
+    VD_PDL_WAIT();
+    __shared__ double sh[32];
+    const GridDev& g = P.g;
+    const long long N = g.ncell();
+    const int n = g.n[d], per = g.per[d];
+    // the line's other two axes: da varies fastest between threads (x for
+    // d = y, z: coalesced)
+    const int da = d == 0 ? 1 : 0, db = d == 2 ? 1 : 2;
+    const long long sd = d == 0 ? 1LL : (d == 1 ? (long long)g.n[0] : (long long)g.n[0] * g.n[1]);
+    const long long lines = (long long)g.n[da] * g.n[db];
+    const double* __restrict__ E = P.S + (EFX_ID + d) * N;
+    const int nf = per ? n : n + 1; // the periodic wrap face is face 0
+    double gm = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < lines * P.nt;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        const int s = (int)(t / lines);
+        const long long l = t - s * lines;
+        int c[3];
+        c[d] = 0;
+        c[da] = (int)(l % g.n[da]);
+        c[db] = (int)(l / g.n[da]);
+        const long long base = g.idx(c[0], c[1], c[2]);
+        const double* __restrict__ us = u + s * N;
+        const double* __restrict__ ms = P.mu + s * N;
+        const double* __restrict__ ls = lam + s * N;
+        const double* __restrict__ dms = P.dmu + s * N;
+        double* __restrict__ as = adj + s * N;
+        const bool wlo = adj_wall(P, s, d, false), whi = adj_wall(P, s, d, true);
+        const bool elec = s == P.eslot;
+        double wu[6], wv[6], au[6], av[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m)
+        {
+            const long long q = base + clampi(m - 3, n, per) * sd;
+            wu[m] = us[q];
+            wv[m] = ms[q] * E[q];
+            au[m] = av[m] = 0.0;
+        }
+        // lambda of the cells left and right of face f (0 outside a wall)
+        double lL = per ? ls[base + (long long)(n - 1) * sd] : 0.0;
+        double lR = ls[base];
+        for (int f = 0; f < nf; ++f)
+        {
+            int rc[6], dir[6];
+#pragma unroll
+            for (int m = 0; m < 6; ++m)
+            {
+                rc[m] = clampi(f - 3 + m, n, per);
+                dir[m] = m;
+#pragma unroll
+                for (int q = m - 1; q >= 0; --q)
+                    if (rc[q] == rc[m]) dir[m] = dir[q];
+            }
+            const bool wall = (f == 0 && wlo) || (f == n && whi);
+            const double w = P.dt * (lR - lL) / P.dx[d];
+            // no stencil position clamped or wrapped onto another's cell: the
+            // gradient with constant slots (its arrays stay in registers)
+            const bool inner = per ? n >= 6 : (f >= 3 && f + 2 < n);
+            if (!wall && w != 0.0 && inner)
+            {
+                double gu[6], gv[6];
+                weno_face_flux_grad<true>(wu, wv, dir, P.weno_scheme, gu, gv);
+#pragma unroll
+                for (int m = 0; m < 6; ++m)
+                {
+                    au[m] += w * gu[m];
+                    av[m] += w * gv[m];
+                }
+            } else if (!wall && w != 0.0)
+            {
+                double gu[6], gv[6];
+                weno_face_flux_grad<false>(wu, wv, dir, P.weno_scheme, gu, gv);
+#pragma unroll
+                for (int m = 0; m < 6; ++m)
+                    if (dir[m] == m)
+                    {
+                        au[m] += w * gu[m];
+                        av[m] += w * gv[m];
+                    }
+            }
+            // virtual cell f-3 leaves the stencil; f+3 enters
+            adj_line_flush(as, adjnd, dms, E, base + rc[0] * sd, au[0], av[0], wv[0], elec, gm);
+#pragma unroll
+            for (int m = 0; m < 5; ++m)
+            {
+                wu[m] = wu[m + 1];
+                wv[m] = wv[m + 1];
+                au[m] = au[m + 1];
+                av[m] = av[m + 1];
+            }
+            const long long q = base + clampi(f + 3, n, per) * sd;
+            wu[5] = us[q];
+            wv[5] = ms[q] * E[q];
+            au[5] = av[5] = 0.0;
+            lL = lR;
+            lR = (f + 1 < n) ? ls[base + (long long)(f + 1) * sd] : (per ? ls[base] : 0.0);
+        }
+        // virtual cells nf-3 .. nf+1 are still in the window
+#pragma unroll
+        for (int m = 0; m < 5; ++m)
+            adj_line_flush(as, adjnd, dms, E, base + clampi(nf - 3 + m, n, per) * sd, au[m],
+                           av[m], wv[m], elec, gm);
     }
     gm = block_sum(gm, sh);
     if (threadIdx.x == 0 && gm != 0.0) atomicAdd(gmob, gm / P.mob_scale);

@@ -30,6 +30,17 @@ struct Dual
         r.d[k] = 1.0;
         return r;
     }
+    // var() by one select per slot: with k known only at run time the slots
+    // can stay in registers, where the indexed store puts the dual in memory
+    VD_HD static Dual var_sel(double x, int k)
+    {
+        Dual r(x);
+#ifdef __CUDA_ARCH__
+#pragma unroll
+#endif
+        for (int i = 0; i < N; ++i) r.d[i] = (i == k) ? 1.0 : 0.0;
+        return r;
+    }
     VD_HD Dual& operator+=(const Dual& o)
     {
         v += o.v;

@@ -2070,6 +2070,10 @@ void adj_run(Ctx& c, int nsteps, int K)
     // lambda = dJ/du at the last step: dV on the electrons
     VD_CUDA_OK(cudaMemsetAsync(a.lam, 0, sizeof(double) * (size_t)a.nt * N, c.st));
     LAUNCH(k_fill<double>, gsz(N), BS, c.st, a.lam + (size_t)a.eslot * N, adj_cell_volume(c), N);
+    // WENO faces by line march (k_adj_faces_line); VD_ADJ_FACES_LINE=0 keeps
+    // one thread per face (k_adj_faces; tests compare the two)
+    const char* le = std::getenv("VD_ADJ_FACES_LINE");
+    const bool lines = P.hyp_order > 2 && !(le && le[0] == '0');
     std::vector<double*> t(ntraj);
     for (int b = nck - 1; b >= 0; --b)
     {
@@ -2088,6 +2092,12 @@ void adj_run(Ctx& c, int nsteps, int K)
             VD_CUDA_OK(cudaMemsetAsync(a.adjnd, 0, sizeof(double) * N, c.st));
             for (int d = 0; d < c.cfg.dim; ++d)
             {
+                if (lines)
+                {
+                    LAUNCH(k_adj_faces_line, gsz128(N / c.g.n[d] * a.nt), 128, c.st, P, d, uk,
+                           a.lam, a.adj, a.adjnd, a.acc + 1 + ADJ_NR);
+                    continue;
+                }
                 const long long nf = N / c.g.n[d] * (c.g.n[d] + 1);
                 LAUNCH(k_adj_faces, gsz128(nf), 128, c.st, P, d, uk, a.lam, a.adj, a.adjnd,
                        a.acc + 1 + ADJ_NR);
