@@ -336,6 +336,103 @@ __global__ void __launch_bounds__(256) k_adj_step(AdjParams P, const double* __r
     }
 }
 
+// The same step in two parts, each face flux computed once.  Part 1, the
+// chemistry: unew = u + dt N_A wdot(u).
+__global__ void __launch_bounds__(256) k_adj_chem_step(AdjParams P, const double* __restrict__ u,
+                                                       double* __restrict__ unew)
+{
+    VD_PDL_WAIT();
+    const long long N = P.g.ncell();
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        double C[NUM_SPECIES], q[NUM_REACTIONS], W[NUM_SPECIES];
+        int slot = 0;
+        for (int sp = 0; sp < NUM_SPECIES; ++sp)
+        {
+            const bool tr = slot < P.nt && P.spec[slot] == sp;
+            C[sp] = (tr ? u[slot * N + t] : P.S[sp * N + t]) / N_A;
+            if (tr) ++slot;
+        }
+        mech_rates<double>(P.Tg, C, P.S[ETEMP_ID * N + t], P.theta, q);
+        mech_wdot<double>(q, W);
+        for (int s = 0; s < P.nt; ++s) unew[s * N + t] = u[s * N + t] + P.dt * (W[P.spec[s]] * N_A);
+    }
+}
+
+// Part 2, direction d: unew += dt (F_lo - F_hi)/dx_d, one thread per line of
+// cells along d and species, marching the faces with the six stencil cells'
+// u, v in registers (ghost positions clamped or wrapped as in k_adj_step);
+// each face's flux is formed once and closes the cell on its left.  The
+// periodic wrap face n is face 0, whose flux the thread keeps.
+__global__ void __launch_bounds__(128) k_adj_flux_line(AdjParams P, int d,
+                                                       const double* __restrict__ u,
+                                                       double* __restrict__ unew)
+{
+    VD_PDL_WAIT();
+    const GridDev& g = P.g;
+    const long long N = g.ncell();
+    const int n = g.n[d], per = g.per[d];
+    const int da = d == 0 ? 1 : 0, db = d == 2 ? 1 : 2;
+    const long long sd = d == 0 ? 1LL : (d == 1 ? (long long)g.n[0] : (long long)g.n[0] * g.n[1]);
+    const long long lines = (long long)g.n[da] * g.n[db];
+    const double* __restrict__ E = P.S + (EFX_ID + d) * N;
+    const double cdt = P.dt / P.dx[d];
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < lines * P.nt;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        const int s = (int)(t / lines);
+        const long long l = t - s * lines;
+        int c[3];
+        c[d] = 0;
+        c[da] = (int)(l % g.n[da]);
+        c[db] = (int)(l / g.n[da]);
+        const long long base = g.idx(c[0], c[1], c[2]);
+        const double* __restrict__ us = u + s * N;
+        const double* __restrict__ ms = P.mu + s * N;
+        double* __restrict__ un = unew + s * N;
+        const bool wlo = adj_wall(P, s, d, false), whi = adj_wall(P, s, d, true);
+        double wu[6], wv[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m)
+        {
+            const long long q = base + clampi(m - 3, n, per) * sd;
+            wu[m] = us[q];
+            wv[m] = ms[q] * E[q];
+        }
+        double F0 = 0.0, Fprev = 0.0;
+        for (int f = 0; f <= n; ++f)
+        {
+            double F;
+            if (per && f == n)
+                F = F0;
+            else
+            {
+                F = face_flux6(wu, wv, P.hyp_order, P.weno_scheme, P.dxmin, P.dt);
+                if ((f == 0 && wlo) || (f == n && whi)) F = 0.0;
+            }
+            if (f == 0)
+                F0 = F;
+            else
+            {
+                const long long q = base + (long long)(f - 1) * sd;
+                un[q] += cdt * (Fprev - F);
+            }
+            Fprev = F;
+            if (f == n) break;
+#pragma unroll
+            for (int m = 0; m < 5; ++m)
+            {
+                wu[m] = wu[m + 1];
+                wv[m] = wv[m + 1];
+            }
+            const long long q = base + clampi(f + 3, n, per) * sd;
+            wu[5] = us[q];
+            wv[5] = ms[q] * E[q];
+        }
+    }
+}
+
 // Adjoint of the face fluxes of direction d: one thread per face.
 __global__ void __launch_bounds__(128) k_adj_faces(AdjParams P, int d,
                                                    const double* __restrict__ u,

@@ -2003,7 +2003,18 @@ AdjParams adj_params(Ctx& c, AdjState& a)
 void adj_step(Ctx& c, const AdjParams& P, const double* from, double* to)
 {
     LAUNCH(k_adj_props, gsz(c.N), BS, c.st, P, from);
-    LAUNCH(k_adj_step, gsz(c.N), BS, c.st, P, from, to);
+    // chemistry, then one line march per direction with each face flux
+    // formed once; VD_ADJ_STEP_LINE=0 keeps one thread per cell forming
+    // both of its faces (k_adj_step; tests compare the two)
+    const char* e = std::getenv("VD_ADJ_STEP_LINE");
+    if (e && e[0] == '0')
+    {
+        LAUNCH(k_adj_step, gsz(c.N), BS, c.st, P, from, to);
+        return;
+    }
+    LAUNCH(k_adj_chem_step, gsz(c.N), BS, c.st, P, from, to);
+    for (int d = 0; d < c.cfg.dim; ++d)
+        LAUNCH(k_adj_flux_line, gsz128(c.N / c.g.n[d] * P.nt), 128, c.st, P, d, from, to);
 }
 
 double adj_cell_volume(const Ctx& c)
