@@ -229,6 +229,35 @@ def test_adjoint_step_line_march(require_gpu, monkeypatch, kind, hyp):
     assert worst <= 1e-9, worst
 
 
+# Lines split into segments (the launch's own choice: 8 at these sizes, and
+# 3) against whole lines: the forward map's segments each form their own
+# faces, so the state is the same bit for bit; the adjoint's seam cells take
+# atomic adds from two segments, so the gradient agrees to rounding.
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["box", "periodic_walled", "2d"])
+def test_adjoint_line_segments(require_gpu, monkeypatch, kind):
+    cfg, S = line_case(kind)
+    p = params(7)
+    out = []
+    for v in ("1", None, "3"):
+        if v is None:
+            monkeypatch.delenv("VD_ADJ_LINE_SEGMENTS", raising=False)
+        else:
+            monkeypatch.setenv("VD_ADJ_LINE_SEGMENTS", v)
+        g = vb.Vidyut(cfg)
+        g.set_state(0, S)
+        g.adjoint_set_params(p)
+        J, u = g.adjoint_forward(5, species=True)
+        out.append((J, u, g.adjoint_run(5, K=2)))
+        g.close()
+    J1, u1, (_, g1) = out[0]
+    for J, u, (Ja, gr) in out[1:]:
+        assert J == J1 and Ja == J1
+        assert np.array_equal(u, u1)
+        worst, _ = grad_close(gr, g1, 1e-12)
+        assert worst <= 1e-12, worst
+
+
 @pytest.mark.gpu
 def test_adjoint_checkpoint_intervals(require_gpu):
     cfg, S = small_case()

@@ -360,12 +360,15 @@ __global__ void __launch_bounds__(256) k_adj_chem_step(AdjParams P, const double
     }
 }
 
-// Part 2, direction d: unew += dt (F_lo - F_hi)/dx_d, one thread per line of
-// cells along d and species, marching the faces with the six stencil cells'
-// u, v in registers (ghost positions clamped or wrapped as in k_adj_step);
-// each face's flux is formed once and closes the cell on its left.  The
-// periodic wrap face n is face 0, whose flux the thread keeps.
-__global__ void __launch_bounds__(128) k_adj_flux_line(AdjParams P, int d,
+// Part 2, direction d: unew += dt (F_lo - F_hi)/dx_d, one thread per
+// segment of a line of cells along d and species (nseg segments a line, so
+// that the launch fills its last wave), marching the faces with the six
+// stencil cells' u, v in registers (ghost positions clamped or wrapped as in
+// k_adj_step); each face's flux is formed once and closes the cell on its
+// left.  A segment of cells c0..c1-1 forms faces c0..c1 (one face more than
+// its cells, shared with the next segment) and is the only writer of its
+// cells.
+__global__ void __launch_bounds__(128) k_adj_flux_line(AdjParams P, int d, int nseg,
                                                        const double* __restrict__ u,
                                                        double* __restrict__ unew)
 {
@@ -378,11 +381,14 @@ __global__ void __launch_bounds__(128) k_adj_flux_line(AdjParams P, int d,
     const long long lines = (long long)g.n[da] * g.n[db];
     const double* __restrict__ E = P.S + (EFX_ID + d) * N;
     const double cdt = P.dt / P.dx[d];
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < lines * P.nt;
-         t += (long long)gridDim.x * blockDim.x)
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+         t < lines * nseg * P.nt; t += (long long)gridDim.x * blockDim.x)
     {
-        const int s = (int)(t / lines);
-        const long long l = t - s * lines;
+        const int s = (int)(t / (lines * nseg));
+        const long long r = t - s * lines * nseg;
+        const int seg = (int)(r / lines);
+        const long long l = r - seg * lines;
+        const int c0 = (int)((long long)seg * n / nseg), c1 = (int)((long long)(seg + 1) * n / nseg);
         int c[3];
         c[d] = 0;
         c[da] = (int)(l % g.n[da]);
@@ -396,30 +402,22 @@ __global__ void __launch_bounds__(128) k_adj_flux_line(AdjParams P, int d,
 #pragma unroll
         for (int m = 0; m < 6; ++m)
         {
-            const long long q = base + clampi(m - 3, n, per) * sd;
+            const long long q = base + clampi(c0 - 3 + m, n, per) * sd;
             wu[m] = us[q];
             wv[m] = ms[q] * E[q];
         }
-        double F0 = 0.0, Fprev = 0.0;
-        for (int f = 0; f <= n; ++f)
+        double Fprev = 0.0;
+        for (int f = c0; f <= c1; ++f)
         {
-            double F;
-            if (per && f == n)
-                F = F0;
-            else
-            {
-                F = face_flux6(wu, wv, P.hyp_order, P.weno_scheme, P.dxmin, P.dt);
-                if ((f == 0 && wlo) || (f == n && whi)) F = 0.0;
-            }
-            if (f == 0)
-                F0 = F;
-            else
+            double F = face_flux6(wu, wv, P.hyp_order, P.weno_scheme, P.dxmin, P.dt);
+            if ((f == 0 && wlo) || (f == n && whi)) F = 0.0;
+            if (f > c0)
             {
                 const long long q = base + (long long)(f - 1) * sd;
                 un[q] += cdt * (Fprev - F);
             }
             Fprev = F;
-            if (f == n) break;
+            if (f == c1) break;
 #pragma unroll
             for (int m = 0; m < 5; ++m)
             {
@@ -551,16 +549,22 @@ __device__ __forceinline__ void adj_line_flush(double* __restrict__ as, double* 
                                                const double* __restrict__ dms,
                                                const double* __restrict__ E, long long q,
                                                double au, double av, double v, bool elec,
-                                               double& gm)
+                                               bool seam, double& gm)
 {
-    if (au != 0.0) as[q] += au;
+    if (au != 0.0)
+    {
+        if (seam)
+            atomicAdd(&as[q], au);
+        else
+            as[q] += au;
+    }
     if (av == 0.0) return;
     const double dn = dms[q] * E[q];
     if (dn != 0.0) atomicAdd(&adjnd[q], av * dn);
     if (elec) gm += av * v;
 }
 
-__global__ void __launch_bounds__(128) k_adj_faces_line(AdjParams P, int d,
+__global__ void __launch_bounds__(128) k_adj_faces_line(AdjParams P, int d, int nseg,
                                                         const double* __restrict__ u,
                                                         const double* __restrict__ lam,
                                                         double* __restrict__ adj,
@@ -579,11 +583,18 @@ __global__ void __launch_bounds__(128) k_adj_faces_line(AdjParams P, int d,
     const double* __restrict__ E = P.S + (EFX_ID + d) * N;
     const int nf = per ? n : n + 1; // the periodic wrap face is face 0
     double gm = 0.0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < lines * P.nt;
-         t += (long long)gridDim.x * blockDim.x)
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+         t < lines * nseg * P.nt; t += (long long)gridDim.x * blockDim.x)
     {
-        const int s = (int)(t / lines);
-        const long long l = t - s * lines;
+        const int s = (int)(t / (lines * nseg));
+        const long long r = t - s * lines * nseg;
+        const int seg = (int)(r / lines);
+        const long long l = r - seg * lines;
+        // faces f0..f1-1 of the line; the five cells at either end of the
+        // segment also take contributions from the neighbouring segments
+        // (through the wrap in periodic lines): atomic adds there
+        const int f0 = (int)((long long)seg * nf / nseg), f1 = (int)((long long)(seg + 1) * nf / nseg);
+        const bool seams = nseg > 1;
         int c[3];
         c[d] = 0;
         c[da] = (int)(l % g.n[da]);
@@ -600,15 +611,15 @@ __global__ void __launch_bounds__(128) k_adj_faces_line(AdjParams P, int d,
 #pragma unroll
         for (int m = 0; m < 6; ++m)
         {
-            const long long q = base + clampi(m - 3, n, per) * sd;
+            const long long q = base + clampi(f0 - 3 + m, n, per) * sd;
             wu[m] = us[q];
             wv[m] = ms[q] * E[q];
             au[m] = av[m] = 0.0;
         }
         // lambda of the cells left and right of face f (0 outside a wall)
-        double lL = per ? ls[base + (long long)(n - 1) * sd] : 0.0;
-        double lR = ls[base];
-        for (int f = 0; f < nf; ++f)
+        double lL = (f0 > 0 || per) ? ls[base + (long long)clampi(f0 - 1, n, per) * sd] : 0.0;
+        double lR = (f0 < n) ? ls[base + (long long)f0 * sd] : 0.0;
+        for (int f = f0; f < f1; ++f)
         {
             int rc[6], dir[6];
 #pragma unroll
@@ -648,7 +659,8 @@ __global__ void __launch_bounds__(128) k_adj_faces_line(AdjParams P, int d,
                     }
             }
             // virtual cell f-3 leaves the stencil; f+3 enters
-            adj_line_flush(as, adjnd, dms, E, base + rc[0] * sd, au[0], av[0], wv[0], elec, gm);
+            adj_line_flush(as, adjnd, dms, E, base + rc[0] * sd, au[0], av[0], wv[0], elec,
+                           seams && f - f0 < 5, gm);
 #pragma unroll
             for (int m = 0; m < 5; ++m)
             {
@@ -664,11 +676,11 @@ __global__ void __launch_bounds__(128) k_adj_faces_line(AdjParams P, int d,
             lL = lR;
             lR = (f + 1 < n) ? ls[base + (long long)(f + 1) * sd] : (per ? ls[base] : 0.0);
         }
-        // virtual cells nf-3 .. nf+1 are still in the window
+        // virtual cells f1-3 .. f1+1 are still in the window
 #pragma unroll
         for (int m = 0; m < 5; ++m)
-            adj_line_flush(as, adjnd, dms, E, base + clampi(nf - 3 + m, n, per) * sd, au[m],
-                           av[m], wv[m], elec, gm);
+            adj_line_flush(as, adjnd, dms, E, base + clampi(f1 - 3 + m, n, per) * sd, au[m],
+                           av[m], wv[m], elec, seams, gm);
     }
     gm = block_sum(gm, sh);
     if (threadIdx.x == 0 && gm != 0.0) atomicAdd(gmob, gm / P.mob_scale);

@@ -1938,6 +1938,35 @@ dim3 gsz128(long long n)
     return dim3((unsigned)b);
 }
 
+// Segments a line for the line-march kernels (128-thread blocks, one thread
+// per segment of a line and species): whole lines leave the launch's last
+// wave part-empty (128^3, 7 species: 3.03 waves of the face adjoint at 2
+// blocks per SM), shorter segments fill it at the cost of the faces a
+// segment forms twice or the window it loads first.  Model: waves x (faces
+// a segment + 1) at the occupancy the kernel reaches; VD_ADJ_LINE_SEGMENTS
+// fixes the count (tests).
+template <typename K>
+int line_segments(K kernel, long long lines, int nf)
+{
+    if (const char* e = std::getenv("VD_ADJ_LINE_SEGMENTS"))
+        return std::max(1, std::atoi(e));
+    int occ = 0;
+    VD_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 128, 0));
+    const double slots = (double)std::max(occ, 1) * sm_count() * 128;
+    int best = 1;
+    double bc = 1e300;
+    for (int S = 1; S <= 8; ++S)
+    {
+        const double cost = std::ceil((double)lines * S / slots) * ((double)nf / S + 1.0);
+        if (cost < bc * (1.0 - 1e-9))
+        {
+            bc = cost;
+            best = S;
+        }
+    }
+    return best;
+}
+
 AdjState& adj_state(Ctx& c, int slots)
 {
     const long long N = c.N;
@@ -2014,7 +2043,11 @@ void adj_step(Ctx& c, const AdjParams& P, const double* from, double* to)
     }
     LAUNCH(k_adj_chem_step, gsz(c.N), BS, c.st, P, from, to);
     for (int d = 0; d < c.cfg.dim; ++d)
-        LAUNCH(k_adj_flux_line, gsz128(c.N / c.g.n[d] * P.nt), 128, c.st, P, d, from, to);
+    {
+        const long long lines = c.N / c.g.n[d] * P.nt;
+        const int nseg = line_segments(k_adj_flux_line, lines, c.g.n[d] + 1);
+        LAUNCH(k_adj_flux_line, gsz128(lines * nseg), 128, c.st, P, d, nseg, from, to);
+    }
 }
 
 double adj_cell_volume(const Ctx& c)
@@ -2084,7 +2117,7 @@ void adj_run(Ctx& c, int nsteps, int K)
     // WENO faces by line march (k_adj_faces_line); VD_ADJ_FACES_LINE=0 keeps
     // one thread per face (k_adj_faces; tests compare the two)
     const char* le = std::getenv("VD_ADJ_FACES_LINE");
-    const bool lines = P.hyp_order > 2 && !(le && le[0] == '0');
+    const bool line_faces = P.hyp_order > 2 && !(le && le[0] == '0');
     std::vector<double*> t(ntraj);
     for (int b = nck - 1; b >= 0; --b)
     {
@@ -2103,9 +2136,11 @@ void adj_run(Ctx& c, int nsteps, int K)
             VD_CUDA_OK(cudaMemsetAsync(a.adjnd, 0, sizeof(double) * N, c.st));
             for (int d = 0; d < c.cfg.dim; ++d)
             {
-                if (lines)
+                if (line_faces)
                 {
-                    LAUNCH(k_adj_faces_line, gsz128(N / c.g.n[d] * a.nt), 128, c.st, P, d, uk,
+                    const long long lines = N / c.g.n[d] * a.nt;
+                    const int nseg = line_segments(k_adj_faces_line, lines, c.g.n[d] + 1);
+                    LAUNCH(k_adj_faces_line, gsz128(lines * nseg), 128, c.st, P, d, nseg, uk,
                            a.lam, a.adj, a.adjnd, a.acc + 1 + ADJ_NR);
                     continue;
                 }
