@@ -13,13 +13,19 @@
 // mechanism with the log pre-factors shifted by theta (A_r -> A_r e^theta_r).
 // Objective J = sum over cells of n_e dV after the last step.
 //
+// The forward step runs as the chemistry (k_adj_chem_step) and one line
+// march per direction (k_adj_flux_line: each face flux formed once); the
+// one-kernel form k_adj_step is kept for comparison.
+//
 // Backward step k (lambda = dJ/du^{k+1}, states recomputed from checkpoints):
 //     lambda <- lambda + dt (dR/du)^T lambda,   g <- g + dt (dR/dp)^T lambda
-// evaluated at u^k.  One thread per face differentiates its flux -- WENO:
+// evaluated at u^k.  WENO: one thread per segment of a line of faces and
+// species marches the faces (k_adj_faces_line), differentiates each flux
 // from the 5-slot dual gradient of each of its four reconstructions
-// (weno_face_flux_grad); upwind and WAF: dual numbers, one pass for the
-// stencil densities and one for the velocities -- and scatters w dF/du_m
-// with FP64 atomics, w = dt (lambda_R - lambda_L)/dx.
+// (weno_face_flux_grad) and writes each cell's sum of w dF/du_m once,
+// w = dt (lambda_R - lambda_L)/dx.  Upwind and WAF: one thread per face
+// (k_adj_faces), dual numbers, one pass for the stencil densities and one
+// for the velocities, scattered with FP64 atomics.
 // Stencil positions that clamp onto the same boundary cell are seeded as one
 // direction: the WENO smoothness indicators of such a flat sub-stencil are
 // zero only up to rounding, and per-position derivatives of that rounding
