@@ -231,8 +231,9 @@ __device__ __forceinline__ void weno_face_flux_grad(const double* u, const doubl
 
 // columns of the chemistry Jacobian formed per dual pass (k_adj_chem_update):
 // each pass recomputes the rate exponentials, more slots cost registers;
-// measured at 128^3 / 50 steps (LMEA): 1, 2, 4, 8 slots 1033, 1002, 1048,
-// 1038 ms per adjoint run
+// measured at 128^3 / 50 steps (LMEA): 1, 2, 3 slots 545, 513, 513 ms per
+// adjoint run (1, 2, 4, 8 slots 1033, 1002, 1048, 1038 ms with the earlier
+// face and step kernels)
 #ifndef VD_ADJ_CHEM_SLOTS
 #define VD_ADJ_CHEM_SLOTS 2
 #endif
@@ -705,9 +706,11 @@ __global__ void __launch_bounds__(128) k_adj_chem_update(AdjParams P,
 {
     VD_PDL_WAIT();
     __shared__ double sh[32];
+    // the thread's pre-factor gradient sums, in shared memory: 30 registers
+    // pairs fewer for the dual passes
+    __shared__ double gl[NUM_REACTIONS][128];
+    for (int r = 0; r < NUM_REACTIONS; ++r) gl[r][threadIdx.x] = 0.0;
     const long long N = P.g.ncell();
-    double gl[NUM_REACTIONS];
-    for (int r = 0; r < NUM_REACTIONS; ++r) gl[r] = 0.0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N;
          t += (long long)gridDim.x * blockDim.x)
     {
@@ -726,7 +729,7 @@ __global__ void __launch_bounds__(128) k_adj_chem_update(AdjParams P,
             double q[NUM_REACTIONS], ln[NUM_REACTIONS];
             mech_rates<double>(P.Tg, Cv, te, P.theta, q);
             mech_lam_nu(lamc, ln);
-            for (int r = 0; r < NUM_REACTIONS; ++r) gl[r] += P.dt * N_A * q[r] * ln[r];
+            for (int r = 0; r < NUM_REACTIONS; ++r) gl[r][threadIdx.x] += P.dt * N_A * q[r] * ln[r];
         }
         // dR_s/du_s2 = d wdot_s / d C_s2 (R = N_A wdot, C = u / N_A),
         // VD_ADJ_CHEM_SLOTS columns per pass
@@ -735,8 +738,16 @@ __global__ void __launch_bounds__(128) k_adj_chem_update(AdjParams P,
         for (int s0 = 0; s0 < P.nt; s0 += K)
         {
             Dual<K> C[NUM_SPECIES], q[NUM_REACTIONS], W[NUM_SPECIES];
-            for (int sp = 0; sp < NUM_SPECIES; ++sp) C[sp] = Dual<K>(Cv[sp]);
-            for (int e = 0; e < K && s0 + e < P.nt; ++e) C[P.spec[s0 + e]].d[e] = 1.0;
+            // seeds by selects (an index known only at run time would put
+            // the duals in local memory)
+#pragma unroll
+            for (int sp = 0; sp < NUM_SPECIES; ++sp)
+            {
+                C[sp] = Dual<K>(Cv[sp]);
+#pragma unroll
+                for (int e = 0; e < K; ++e)
+                    if (s0 + e < P.nt && P.spec[s0 + e] == sp) C[sp].d[e] = 1.0;
+            }
             mech_rates<Dual<K>>(P.Tg, C, te, P.theta, q);
             mech_wdot<Dual<K>>(q, W);
             for (int e = 0; e < K && s0 + e < P.nt; ++e)
@@ -744,13 +755,14 @@ __global__ void __launch_bounds__(128) k_adj_chem_update(AdjParams P,
                 const int s2 = s0 + e;
                 double a = 0.0;
                 for (int sp = 0; sp < NUM_SPECIES; ++sp) a += lamc[sp] * W[sp].d[e];
-                lam[s2 * N + t] = lamc[P.spec[s2]] + P.dt * a + adj[s2 * N + t] + nd;
+                // lamc[P.spec[s2]], read back from memory (not yet rewritten)
+                lam[s2 * N + t] = lam[s2 * N + t] + P.dt * a + adj[s2 * N + t] + nd;
             }
         }
     }
     for (int r = 0; r < NUM_REACTIONS; ++r)
     {
-        const double v = block_sum(gl[r], sh);
+        const double v = block_sum(gl[r][threadIdx.x], sh);
         if (threadIdx.x == 0 && v != 0.0) atomicAdd(&gtheta[r], v);
     }
 }
