@@ -571,7 +571,13 @@ __device__ __forceinline__ void adj_line_flush(double* __restrict__ as, double* 
     if (elec) gm += av * v;
 }
 
-__global__ void __launch_bounds__(128) k_adj_faces_line(AdjParams P, int d, int nseg,
+// Blocks per SM the face adjoint's registers are sized for: 3 (168
+// registers, about 0.5 KB of spills) beats 2 (242, none) and 4 (128, 1.2 KB)
+// at 128^3: 496, 510, 521 ms per adjoint run.
+#ifndef VD_ADJ_FACES_MINB
+#define VD_ADJ_FACES_MINB 3
+#endif
+__global__ void __launch_bounds__(128, VD_ADJ_FACES_MINB) k_adj_faces_line(AdjParams P, int d, int nseg,
                                                         const double* __restrict__ u,
                                                         const double* __restrict__ lam,
                                                         double* __restrict__ adj,
