@@ -24,7 +24,12 @@ Checks, all FP64:
   relative (test_adjoint_c4_vs_fd);
 * checkpoint intervals that do and do not divide the step count give the same
   gradient; the same checks through a torch.autograd.Function wrapper (test
-  harness only).
+  harness only);
+* the line-march kernels against the one-thread-per-face and per-cell forms
+  they replace (VD_ADJ_FACES_LINE=0, VD_ADJ_STEP_LINE=0) and across segment
+  counts (VD_ADJ_LINE_SEGMENTS), on a box, a periodic direction with
+  flux-zeroing walls, and 2-D, each also against the oracle's tangent-linear
+  gradient.
 """
 import numpy as np
 import pytest
